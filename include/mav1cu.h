@@ -1,0 +1,211 @@
+/*
+ * mav1cu — B200 (sm_100a) encode backend for the mav1 AV1 encoder.
+ *
+ * C ABI of libmav1cu.so: plain pointers, sizes and status codes; no CUDA or
+ * C++ types cross it (a CUDA stream is passed as void *). One session holds
+ * the device-resident state of one encoder instance: its frame buffers,
+ * reference pictures, analysis tables and stage outputs, laid out exactly as
+ * the reference encoder's shared buffers so the host entropy coder reads
+ * them unchanged.
+ *
+ * The stage entry points are the hooks of the reference's backend vtable
+ * (src/backend.h:10-24 of neolite/mav1-encoder) plus the host helpers of its
+ * frame driver that run on the device here; each cites the reference
+ * function it replaces. Stage calls are asynchronous on the session's stream
+ * and return MAV1CU_OK once enqueued; errors are sticky per session
+ * (mav1cu_error_string) and reported by the next call.
+ */
+#ifndef MAV1CU_H
+#define MAV1CU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- record formats shared with the host encoder ------------------------
+ * Byte-identical to the reference's structs (the host tile writer reads
+ * them): FrameParams src/kernels/k_common.h:52-85 (392 bytes), BlockInfo
+ * k_common.h:98-120 (108 bytes), SbInfo k_common.h:123-128 (356 bytes),
+ * LrUnit src/kernels/k_lr.h:12-18 (48 bytes). Every field is 32 bits. */
+typedef struct {
+  int32_t mi_cols, mi_rows;
+  int32_t sb_cols, sb_rows;
+  int32_t plane_w[3], plane_h[3];
+  int32_t stride[3], offset[3];
+  int32_t base_q_idx;
+  int32_t dc_q[3], ac_q[3];
+  int32_t frame_is_intra;
+  int32_t reduced_tx_set;
+  int32_t enable_intra_edge_filter;
+  int32_t tx_search;
+  int32_t lambda;
+  int32_t wave;
+  int32_t num_blocks;
+  int32_t frame_w, frame_h;
+  int32_t me_range;
+  int32_t lossless;
+  int32_t tx_mode_select;
+  int32_t tile_w_sb;
+  int32_t fast;
+  int32_t leaf;
+  int32_t depth_thr;
+  int32_t switchable_interp;
+  int32_t golden;
+  int32_t ref2_frame;
+  int32_t compound;
+  int32_t lf_level[4];
+  int32_t lf_sharpness;
+  int32_t cdef_damping, cdef_bits;
+  int32_t cdef_y_pri[8], cdef_y_sec[8], cdef_uv_pri[8], cdef_uv_sec[8];
+  int32_t lr_type[3], lr_unit_size[3], lr_unit_rows[3], lr_unit_cols[3], lr_unit_off[3];
+  int32_t turbo;
+} mav1cu_frame_params;
+
+typedef struct {
+  int32_t mi_row, mi_col, bsize;
+  int32_t is_inter;
+  int32_t y_mode, uv_mode, angle_y, angle_uv;
+  int32_t mv_row, mv_col;
+  int32_t tx_type;
+  int32_t eob[3];
+  int32_t coef_off[3];
+  int32_t cfl_alpha_u, cfl_alpha_v;
+  int32_t tx_depth;
+  int32_t tx_types_lo, tx_types_hi;
+  int32_t interp_filter;
+  int32_t ref_frame;
+  int32_t ref_frame1;
+  int32_t mv1_row, mv1_col;
+} mav1cu_block_info;
+
+typedef struct {
+  int32_t first_block, num_blocks;
+  int32_t sb_row, sb_col;
+  int32_t part[85];
+} mav1cu_sb_info;
+
+typedef struct {
+  int32_t type;
+  int32_t set;
+  int32_t xqd[2];
+  int32_t wiener[2][3];
+  int32_t pad[2];
+} mav1cu_lr_unit;
+
+/* ---- status codes -------------------------------------------------------- */
+enum {
+  MAV1CU_OK = 0,
+  MAV1CU_ERR_ARG = -1,      /* bad argument (size, buffer id, state) */
+  MAV1CU_ERR_CUDA = -2,     /* a CUDA runtime call failed (see mav1cu_error_string) */
+  MAV1CU_ERR_NOMEM = -3,    /* device allocation failed */
+  MAV1CU_ERR_DEVICE = -4,   /* a kernel reported an error through its status word */
+};
+
+/* ---- session buffers (the reference encoder's Bufs, enc_internal.h:81-151) */
+enum {
+  MAV1CU_BUF_SRC = 0,       /* padded source frame, frame_bytes (encoder.c:113-120,297-310) */
+  MAV1CU_BUF_REC,           /* reconstruction, frame_bytes */
+  MAV1CU_BUF_REF,           /* LAST reference picture, frame_bytes */
+  MAV1CU_BUF_GOLD,          /* second reference (GOLDEN / ALTREF), frame_bytes */
+  MAV1CU_BUF_PARAMS,        /* mav1cu_frame_params */
+  MAV1CU_BUF_MATS,          /* forward matrices, 15 x 4096 int32 (fwd_matrices.c:57-65) */
+  MAV1CU_BUF_MVFIELD,       /* int32 [num_sbs][85][2] motion vectors of LAST */
+  MAV1CU_BUF_MVGOLD,        /* int32 [num_sbs][85][2] motion vectors of the second reference */
+  MAV1CU_BUF_BLOCKS,        /* mav1cu_block_info [num_sbs][64] (decode order) */
+  MAV1CU_BUF_SBS,           /* mav1cu_sb_info [num_sbs] */
+  MAV1CU_BUF_COEFS,         /* int32 [num_sbs][6144] quantised levels */
+  MAV1CU_BUF_LFMASK,        /* uint8 [mi_rows][mi_cols]: bsize | skip << 5 | tx_depth << 6 */
+  MAV1CU_BUF_CDEFBUF,       /* num presets x frame_bytes: CDEF output of every preset */
+  MAV1CU_BUF_CDEF_CHOICE,   /* int8 [num_sbs]: chosen CDEF preset */
+  MAV1CU_BUF_DBK,           /* deblocked frame before CDEF, frame_bytes */
+  MAV1CU_BUF_LROUT,         /* loop-restoration output, frame_bytes */
+  MAV1CU_BUF_LRUNITS,       /* mav1cu_lr_unit [3 (sb_rows+1)(sb_cols+1)] */
+  MAV1CU_BUF_ACOSTS,        /* int64 [num_sbs][85*13] analysis pass-1 costs */
+  MAV1CU_BUF_AINFOS,        /* mav1cu_block_info [num_sbs][85*13] analysis pass-1 decisions */
+  MAV1CU_BUF_COUNT
+};
+
+typedef struct mav1cu_session mav1cu_session;
+
+/* Creates a session for frames of width x height on the current CUDA device,
+ * with room for `max_cdef_presets` (0..4) CDEF outputs. Allocates all device
+ * state once (sized like the reference encoder's buffers, encoder.c:124-166).
+ * Replaces backend_metal_create (src/backend.h:37, backend_metal.m:576-610).
+ * Returns MAV1CU_OK and *out, or an error code with a message in err. */
+int mav1cu_session_create(int width, int height, int max_cdef_presets, mav1cu_session **out, char *err,
+                          size_t errlen);
+/* Frees every device resource (Backend.destroy, backend.h:20). */
+void mav1cu_session_destroy(mav1cu_session *s);
+
+/* The CUDA stream (cudaStream_t) the session enqueues on; NULL: its own. */
+int mav1cu_set_stream(mav1cu_session *s, void *stream);
+void *mav1cu_get_stream(mav1cu_session *s);
+
+/* Size in bytes and device address of a session buffer. */
+size_t mav1cu_buf_size(const mav1cu_session *s, int buf);
+void *mav1cu_buf_device(mav1cu_session *s, int buf);
+/* Asynchronous copies between host memory and a session buffer (pinned host
+ * memory makes them truly asynchronous). bytes <= mav1cu_buf_size. */
+int mav1cu_upload(mav1cu_session *s, int buf, const void *host, size_t bytes);
+int mav1cu_download(mav1cu_session *s, int buf, void *host, size_t bytes);
+/* Device-to-device copy between two session buffers (e.g. rec -> ref). */
+int mav1cu_copy(mav1cu_session *s, int dst_buf, int src_buf, size_t bytes);
+
+/* Sets the frame parameters of the next stages: a host copy is kept (launch
+ * shapes depend on it) and the record is uploaded to MAV1CU_BUF_PARAMS. */
+int mav1cu_set_params(mav1cu_session *s, const mav1cu_frame_params *fp);
+
+/* ---- stages (enqueue on the session stream) ------------------------------ */
+/* Motion search of every node of every superblock, all levels, for LAST and
+ * (fp.golden) the second reference: quarter-pel / decimated planes, full-pel
+ * search, sub-pel refinement. Writes MVFIELD / MVGOLD.
+ * Replaces Backend.motion_search (backend.h:12; backend_cpu.c:23-56). */
+int mav1cu_motion_search(mav1cu_session *s);
+/* Mode and partition analysis: pass 1 over every candidate block, pass 2
+ * partition decision and block emission. Writes ACOSTS, AINFOS, BLOCKS, SBS.
+ * Replaces Backend.analyze (backend.h:13; backend_cpu.c:58-74). */
+int mav1cu_analyze(mav1cu_session *s);
+/* Intra edge filter types of every block into BlockInfo.interp_filter bits
+ * 4/5. Replaces the host's edge_filter_types (encoder.c:319-346,399-404). */
+int mav1cu_edge_types(mav1cu_session *s);
+/* Reconstruction in decode order: prediction, forward transform,
+ * quantisation, inverse transform. Writes REC, COEFS and the BlockInfo
+ * recon fields. Replaces Backend.recon (backend.h:14; backend_cpu.c:76-156). */
+int mav1cu_recon(mav1cu_session *s);
+/* ME + analysis + edge types + recon of one frame (Backend.frame_core,
+ * backend.h:21-23); motion search is skipped on intra frames. */
+int mav1cu_frame_core(mav1cu_session *s);
+/* Per-mi loop-filter info into LFMASK. Replaces build_filter_info
+ * (encoder.c:513-526). */
+int mav1cu_filter_info(mav1cu_session *s);
+/* Deblocks REC in place, then writes CDEF output of presets 0..n-1 into
+ * CDEFBUF (Backend.filter, backend.h:15-17; backend_cpu.c:158-177). */
+int mav1cu_filter(mav1cu_session *s, int num_cdef_presets);
+/* Picks every superblock's preset by SSE against SRC, writes CDEF_CHOICE and
+ * copies the chosen output into REC. Replaces cdef_select (encoder.c:530-563). */
+int mav1cu_cdef_select(mav1cu_session *s, int num_cdef_presets);
+/* Loop restoration of REC (CDEF output) with DBK and LRUNITS into LROUT
+ * (Backend.restore, backend.h:18-19; backend_cpu.c:179-188). */
+int mav1cu_restore(mav1cu_session *s);
+
+/* Waits for the session stream; returns the sticky error state. */
+int mav1cu_synchronize(mav1cu_session *s);
+/* Message of the first error (empty string if none). */
+const char *mav1cu_error_string(const mav1cu_session *s);
+/* Number of kernel launches this session has enqueued since creation. */
+int64_t mav1cu_launch_count(const mav1cu_session *s);
+
+/* ---- host helpers (no device work) --------------------------------------- */
+/* Forward transform matrices (Q20), 15 x 4096 int32: least-squares inverses
+ * of the normative inverse kernels. Replaces fwd_build_matrices
+ * (fwd_matrices.c:17-65). */
+void mav1cu_build_fwd_matrices(int32_t *mats);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

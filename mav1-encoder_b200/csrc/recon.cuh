@@ -1,0 +1,663 @@
+// Closed-loop reconstruction (reference src/kernels/k_recon.h,
+// scheduled by src/backend_cpu.c:76-156).
+//
+// Per block in decode order: prediction (inter: 8-tap / compound average /
+// optional 3x3 dual-filter search; intra: per transform block from the
+// reconstructed neighbours with the spec's BlockDecoded availability),
+// forward transform by the Q20 matrices, dead-zone quantisation, eob, and
+// the normative inverse transform added back into `rec`; optional luma
+// transform-type search and intra tx_depth search by 16 * SSE + lambda * bits.
+//
+// B200 mapping. An inter block's prediction reads only reference pictures,
+// so every inter block of the frame is coded in one launch (phase 0: one
+// CTA per superblock, all superblocks at once). Intra blocks read their
+// reconstructed neighbours: they run in superblock waves (phase 1), wave
+// (c - tileStart) + 2r, which orders every superblock after its left and
+// above-right neighbours in its tile column, exactly the reference's
+// dependency; inside a superblock the blocks run in decode order and the
+// inter blocks only mark their BlockDecoded flags. Within a transform block
+// the CTA's 256 threads split the residual, both matrix passes (64-bit
+// accumulation), the quantiser, the eob search (a max over inverse-scan
+// positions), the row / column inverse kernels and the reconstruction.
+#pragma once
+
+#include "common.cuh"
+#include "pred.cuh"
+#include "tx.cuh"
+
+namespace rec {
+
+#define RT 256  // threads per CTA
+#define BD_DIM 18
+#define FWD_SLOT_SIZE 4096
+HD int fwd_slot(int kind, int log2n) { return (kind * 5 + log2n - 2) * FWD_SLOT_SIZE; }
+
+// inverse scan tables: position -> scan index, per (scan class, tx size)
+__constant__ int d_inv_scan_off[3][19];
+__device__ int16_t d_inv_scan[8192];
+
+HD int scan_class(int t) {
+  if (t == V_DCT || t == V_ADST || t == V_FLIPADST) return 1;
+  if (t == H_DCT || t == H_ADST || t == H_FLIPADST) return 2;
+  return 0;
+}
+
+struct Ctx {
+  const FrameParams *fp;
+  const uint8_t *src;
+  uint8_t *rec;
+  const uint8_t *ref, *gold;
+  BlockInfo *blocks;
+  const SbInfo *sbs;
+  int32_t *coefs;
+  const int32_t *mats;
+  int *status;
+};
+
+struct Smem {
+  int32_t resid[64 * 64];  // residual, then the inverse transform's plane
+  int32_t tmp[64 * 32];    // forward row pass output
+  int32_t q[32 * 32];      // levels of the current candidate
+  int32_t qbest[32 * 32];  // levels kept by the tx type search
+  int edge[3][EDGE_LEN];   // AboveRow, LeftCol, filter copy
+  uint8_t bd[3 * BD_DIM * BD_DIM];
+  uint8_t bdsave[BD_DIM * BD_DIM];
+  uint8_t save[64 * 64];
+  long long red[RT / 32 + 1];
+  int sse33[33];
+  BlockInfo blk;
+  int maxLumaW, maxLumaH;
+  int flag;
+};
+
+#define BD(sm, p, y, x) (sm).bd[(p) * BD_DIM * BD_DIM + ((y) + 1) * BD_DIM + ((x) + 1)]
+
+__device__ __forceinline__ long long cta_sum64(long long v, Smem &sm) {
+  for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+  if ((threadIdx.x & 31) == 0) sm.red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  long long s = 0;
+  for (int k = 0; k < RT / 32; k++) s += sm.red[k];
+  __syncthreads();
+  return s;
+}
+__device__ __forceinline__ int cta_max(int v, Smem &sm) {
+  for (int off = 16; off > 0; off >>= 1) v = imax(v, __shfl_xor_sync(0xffffffffu, v, off));
+  if ((threadIdx.x & 31) == 0) sm.red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  int m = 0;
+  for (int k = 0; k < RT / 32; k++) m = imax(m, (int)sm.red[k]);
+  __syncthreads();
+  return m;
+}
+
+struct CtaSync {
+  __device__ void operator()() const { __syncthreads(); }
+};
+
+// Levels of a candidate -> reconstruction residual (spec 7.13.3 with the
+// dequantisation of 7.12.3), into sm.resid (stride 64).
+__device__ void inverse_2d(Smem &sm, const int32_t *q, int txSz, int txType, int dcQ, int acQ) {
+  int lw = T(Tx_Width_Log2)[txSz], lh = T(Tx_Height_Log2)[txSz];
+  int w = 1 << lw, h = 1 << lh, tw = imin(32, w), th = imin(32, h);
+  int rowShift = T(Transform_Row_Shift)[txSz], denom = tx::dq_denom(txSz);
+  int rect = iabs(lw - lh) == 1;
+  int rk = tx::row_kind(txType), ck = tx::col_kind(txType);
+  for (int i = threadIdx.x; i < h; i += RT) {
+    int32_t t[64];
+    int nz = 0;
+    for (int j = 0; j < w; j++) {
+      t[j] = (i < th && j < tw) ? tx::dequant_level(q[i * tw + j], (i == 0 && j == 0) ? dcQ : acQ, denom) : 0;
+      nz |= t[j];
+    }
+    if (!nz) {
+      for (int j = 0; j < w; j++) sm.resid[i * 64 + j] = 0;
+      continue;
+    }
+    if (rect)
+      for (int j = 0; j < w; j++) t[j] = (int32_t)round2l((int64_t)t[j] * 2896, 12);
+    tx::inverse_1d(t, rk, lw, 16);
+    for (int j = 0; j < w; j++) sm.resid[i * 64 + j] = clip3(-(1 << 15), (1 << 15) - 1, round2(t[j], rowShift));
+  }
+  __syncthreads();
+  for (int j = threadIdx.x; j < w; j += RT) {
+    int32_t t[64];
+    for (int i = 0; i < h; i++) t[i] = sm.resid[i * 64 + j];
+    tx::inverse_1d(t, ck, lh, 16);
+    for (int i = 0; i < h; i++) sm.resid[i * 64 + j] = round2(t[i], 4);
+  }
+  __syncthreads();
+}
+
+// Transform, quantise and reconstruct one transform block whose prediction
+// is in `rec` (code_tx_block, k_recon.h:60-173). Returns the eob.
+__device__ int code_tx(const Ctx &c, Smem &sm, const uint8_t *src, uint8_t *rec, int stride, int x, int y, int txSz,
+                       int plane, const int *cands, int numCands, int32_t *coefOut, int *outType, long long *outCost) {
+  const FrameParams *fp = c.fp;
+  int lw = T(Tx_Width_Log2)[txSz], lh = T(Tx_Height_Log2)[txSz];
+  int w = 1 << lw, h = 1 << lh, tw = imin(32, w), th = imin(32, h);
+  int dcQ = fp->dc_q[plane], acQ = fp->ac_q[plane];
+  int tid = threadIdx.x;
+  if (fp->lossless) {
+    // 4x4 Walsh-Hadamard, exact inverse of the spec's (k_fwd.h:112-136); one thread
+    if (tid == 0) {
+      int r[16], t[16];
+      for (int i = 0; i < 4; i++)
+        for (int j = 0; j < 4; j++) r[i * 4 + j] = (int)src[(y + i) * stride + x + j] - (int)rec[(y + i) * stride + x + j];
+      for (int j = 0; j < 4; j++) {
+        int a1 = r[0 * 4 + j], b1 = r[1 * 4 + j], c1 = r[2 * 4 + j], d1 = r[3 * 4 + j];
+        a1 += b1;
+        d1 = d1 - c1;
+        int e1 = (a1 - d1) >> 1;
+        b1 = e1 - b1;
+        c1 = e1 - c1;
+        a1 -= c1;
+        d1 += b1;
+        t[0 * 4 + j] = a1; t[1 * 4 + j] = c1; t[2 * 4 + j] = d1; t[3 * 4 + j] = b1;
+      }
+      for (int i = 0; i < 4; i++) {
+        int a1 = t[i * 4 + 0], b1 = t[i * 4 + 1], c1 = t[i * 4 + 2], d1 = t[i * 4 + 3];
+        a1 += b1;
+        d1 -= c1;
+        int e1 = (a1 - d1) >> 1;
+        b1 = e1 - b1;
+        c1 = e1 - c1;
+        a1 -= c1;
+        d1 += b1;
+        sm.q[i * 4 + 0] = a1; sm.q[i * 4 + 1] = c1; sm.q[i * 4 + 2] = d1; sm.q[i * 4 + 3] = b1;
+      }
+      int eob = 0;
+      const int16_t *inv = d_inv_scan + d_inv_scan_off[0][TX_4X4];
+      for (int k = 0; k < 16; k++) {
+        coefOut[k] = sm.q[k];
+        if (sm.q[k] != 0) eob = imax(eob, inv[k] + 1);
+      }
+      if (eob > 0) {
+        int32_t rr[4][4];
+        for (int i = 0; i < 4; i++) {
+          int32_t tt[4];
+          for (int j = 0; j < 4; j++) tt[j] = tx::dequant_level(sm.q[i * 4 + j], (i == 0 && j == 0) ? dcQ : acQ, 1);
+          tx::iwht(tt, 2);
+          for (int j = 0; j < 4; j++) rr[i][j] = tt[j];
+        }
+        for (int j = 0; j < 4; j++) {
+          int32_t tt[4];
+          for (int i = 0; i < 4; i++) tt[i] = clip3(-(1 << 15), (1 << 15) - 1, rr[i][j]);
+          tx::iwht(tt, 0);
+          for (int i = 0; i < 4; i++) rr[i][j] = tt[i];
+        }
+        for (int i = 0; i < 4; i++)
+          for (int j = 0; j < 4; j++) {
+            int o = (y + i) * stride + x + j;
+            rec[o] = (uint8_t)clip1((int)rec[o] + rr[i][j]);
+          }
+      }
+      sm.flag = eob;
+    }
+    __syncthreads();
+    int eob = sm.flag;
+    __syncthreads();
+    *outType = DCT_DCT;
+    *outCost = 0;
+    return eob;
+  }
+
+  int single = numCands == 1 && !fp->tx_mode_select;
+  int shifts = T(Transform_Row_Shift)[txSz] + 4, rect = iabs(lw - lh) == 1;
+  int denom = tx::dq_denom(txSz);
+  uint64_t invDc = tx::quant_inv(dcQ), invAc = tx::quant_inv(acQ);
+  long long bestCost = -1;
+  int bestType = DCT_DCT, bestEob = 0;
+  int32_t *qsrc = sm.q;  // levels the final reconstruction uses
+  for (int ci = 0; ci < numCands; ci++) {
+    int t = cands[ci];
+    int fud = tx::flip_ud(t), flr = tx::flip_lr(t);
+    for (int k = tid; k < h * w; k += RT) {
+      int i = k >> lw, j = k & (w - 1);
+      int yy = fud ? (h - 1 - i) : i, xx = flr ? (w - 1 - j) : j;
+      int o = (y + yy) * stride + x + xx;
+      sm.resid[i * 64 + j] = (int)src[o] - (int)rec[o];
+    }
+    __syncthreads();
+    const int32_t *Mh = c.mats + fwd_slot(tx::row_kind(t), lw), *Mv = c.mats + fwd_slot(tx::col_kind(t), lh);
+    for (int k = tid; k < h * tw; k += RT) {
+      int i = k / tw, kk = k % tw;
+      const int32_t *r = sm.resid + i * 64, *m = Mh + kk * w;
+      int64_t s = 0;
+      for (int j = 0; j < w; j++) s += (int64_t)r[j] * m[j];
+      sm.tmp[i * 32 + kk] = (int32_t)round2l(s, 16);
+    }
+    __syncthreads();
+    const int16_t *inv = d_inv_scan + d_inv_scan_off[scan_class(t)][txSz];
+    int myEob = 0;
+    for (int k = tid; k < th * tw; k += RT) {
+      int k2 = k / tw, kk = k % tw;
+      const int32_t *m = Mv + k2 * h;
+      int64_t s = 0;
+      for (int i = 0; i < h; i++) s += (int64_t)m[i] * sm.tmp[i * 32 + kk];
+      s = s * ((int64_t)1 << shifts);
+      if (rect) s = round2l(s, 12) * 5793;
+      int v = (int)(s >= 0 ? round2l(s, 20) : -round2l(-s, 20));
+      int first = k == 0;
+      int lv = tx::quant_level(v, first ? dcQ : acQ, first ? 26 : 22, denom, first ? invDc : invAc);
+      sm.q[k] = lv;
+      if (lv != 0) myEob = imax(myEob, inv[k] + 1);
+    }
+    int eob = cta_max(myEob, sm);  // includes the barrier after the quantiser
+    if (single) {
+      if (eob > 0) inverse_2d(sm, sm.q, txSz, t, dcQ, acQ);
+      bestCost = 0;
+      bestType = eob > 0 ? t : DCT_DCT;
+      bestEob = eob;
+      qsrc = sm.q;
+      continue;
+    }
+    long long sse = 0;
+    if (eob > 0) {
+      // keep the residual-free path's SSE source intact: the inverse reuses resid
+      inverse_2d(sm, sm.q, txSz, t, dcQ, acQ);
+      for (int k = tid; k < h * w; k += RT) {
+        int i = k >> lw, j = k & (w - 1);
+        int yy = fud ? (h - 1 - i) : i, xx = flr ? (w - 1 - j) : j;
+        int o = (y + yy) * stride + x + xx;
+        int d = (int)src[o] - clip1((int)rec[o] + sm.resid[i * 64 + j]);
+        sse += d * d;
+      }
+    } else {
+      for (int k = tid; k < h * w; k += RT) {
+        int i = k >> lw, j = k & (w - 1);
+        int d = sm.resid[i * 64 + j];
+        sse += d * d;
+      }
+    }
+    sse = cta_sum64(sse, sm);
+    long long bits = 0;
+    if (eob == 0) {
+      bits = tid == 0 ? 8 : 0;
+    } else {
+      for (int k = tid; k < th * tw; k += RT)
+        if (inv[k] < eob) {
+          int l = iabs(sm.q[k]);
+          bits += l == 0 ? 6 : 8 * (2 + 2 * floor_log2(l));
+        }
+      if (tid == 0) bits += 8 * 6 + 8 * 2 * floor_log2(eob + 1);
+    }
+    bits = cta_sum64(bits, sm);
+    long long cost = sse * 16 + (long long)fp->lambda * bits / 8;
+    if (bestCost < 0 || cost < bestCost) {
+      bestCost = cost;
+      bestType = eob > 0 ? t : DCT_DCT;
+      bestEob = eob;
+      for (int k = tid; k < tw * th; k += RT) sm.qbest[k] = sm.q[k];
+      qsrc = sm.qbest;
+      __syncthreads();
+    }
+  }
+  for (int k = tid; k < tw * th; k += RT) coefOut[k] = qsrc[k];
+  if (bestEob > 0) {
+    int fud = tx::flip_ud(bestType), flr = tx::flip_lr(bestType);
+    if (numCands > 1) inverse_2d(sm, qsrc, txSz, bestType, dcQ, acQ);
+    for (int k = tid; k < h * w; k += RT) {
+      int i = k >> lw, j = k & (w - 1);
+      int yy = fud ? (h - 1 - i) : i, xx = flr ? (w - 1 - j) : j;
+      int o = (y + yy) * stride + x + xx;
+      rec[o] = (uint8_t)clip1((int)rec[o] + sm.resid[i * 64 + j]);
+    }
+  }
+  __syncthreads();
+  *outType = bestType;
+  *outCost = bestCost;
+  return bestEob;
+}
+
+__device__ __forceinline__ void tx_type_set(BlockInfo &b, int idx, int t) {
+  if (idx >= 16) return;
+  int sh = 4 * (idx & 7);
+  if (idx < 8) b.tx_types_lo = (int32_t)(((uint32_t)b.tx_types_lo & ~(15u << sh)) | ((uint32_t)t << sh));
+  else b.tx_types_hi = (int32_t)(((uint32_t)b.tx_types_hi & ~(15u << sh)) | ((uint32_t)t << sh));
+}
+
+// CfL alpha of one chroma transform block: first minimum of the SSE over
+// alpha in [-16, 16] (cfl_best_alpha, k_intra.h:277-313).
+__device__ int cfl_alpha(Smem &sm, const uint8_t *luma, int ls, int startX, int startY, int maxLumaW, int maxLumaH,
+                         int log2W, int log2H, int dcv, const uint8_t *sp, int stride, int excludeZero, int *avgOut) {
+  int w = 1 << log2W, h = 1 << log2H, n = w * h;
+  long long sum = 0;
+  for (int k = threadIdx.x; k < n; k += RT) sum += pred::cfl_luma(luma, ls, startX, startY, maxLumaW, maxLumaH, k >> log2W, k & (w - 1));
+  int avg = round2((int)cta_sum64(sum, sm), log2W + log2H);
+  int sse[33];
+  for (int a = 0; a < 33; a++) sse[a] = 0;
+  for (int k = threadIdx.x; k < n; k += RT) {
+    int i = k >> log2W, j = k & (w - 1);
+    int v = pred::cfl_luma(luma, ls, startX, startY, maxLumaW, maxLumaH, i, j) - avg;
+    int s0 = sp[i * stride + j];
+    for (int a = 0; a < 33; a++) {
+      int d = clip3(0, 255, dcv + round2signed((a - 16) * v, 6)) - s0;
+      sse[a] += d * d;
+    }
+  }
+  if (threadIdx.x < 33) sm.sse33[threadIdx.x] = 0;
+  __syncthreads();
+  for (int a = 0; a < 33; a++) {
+    int v = sse[a];
+    for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+    if ((threadIdx.x & 31) == 0) atomicAdd(&sm.sse33[a], v);
+  }
+  __syncthreads();
+  long long best = -1;
+  int bestA = 0;
+  for (int a = -16; a <= 16; a++) {
+    if (a == 0 && excludeZero) continue;
+    long long s = sm.sse33[a + 16];
+    if (best < 0 || s < best) {
+      best = s;
+      bestA = a;
+    }
+  }
+  __syncthreads();
+  *avgOut = avg;
+  return bestA;
+}
+
+// Every transform block of one plane of block b (code_plane, k_recon.h:190-291).
+__device__ long long code_plane(const Ctx &c, Smem &sm, int plane, int txSz) {
+  const FrameParams *fp = c.fp;
+  BlockInfo &b = sm.blk;
+  int bs = b.bsize, MiRow = b.mi_row, MiCol = b.mi_col;
+  int AvailU = MiRow > 0, AvailL = MiCol > tile_col_start(fp, MiCol);
+  int sub = plane > 0;
+  int planeSz = T(Subsampled_Size)[bs][sub][sub];
+  int num4x4W = T(Num_4x4_Blocks_Wide)[planeSz], num4x4H = T(Num_4x4_Blocks_High)[planeSz];
+  int baseX = (MiCol >> sub) * 4, baseY = (MiRow >> sub) * 4;
+  int stride = fp->stride[plane];
+  uint8_t *px = c.rec + fp->offset[plane];
+  const uint8_t *spx = c.src + fp->offset[plane];
+  int stepX = T(Tx_Width)[txSz] >> 2, stepY = T(Tx_Height)[txSz] >> 2;
+  int cands[16], numCands = 0;
+  int isInter = b.is_inter;
+  if (plane == 0) {
+    int set = get_tx_set(txSz, isInter, fp->reduced_tx_set);
+    if (!fp->tx_search || set == TX_SET_DCTONLY || fp->lossless) {
+      cands[numCands++] = DCT_DCT;
+    } else {
+      for (int t = 0; t < 16; t++)
+        if (tx_type_in_set(set, t, isInter)) cands[numCands++] = t;
+    }
+  } else {
+    cands[numCands++] = chroma_tx_type(txSz, isInter, b.uv_mode, b.tx_type, fp->reduced_tx_set);
+  }
+  long long total = 0;
+  int txIdx = 0, anyNz = 0;
+  int *above = sm.edge[0] + EDGE_OFF, *left = sm.edge[1] + EDGE_OFF, *etmp = sm.edge[2];
+  for (int y = 0; y < num4x4H; y += stepY) {
+    for (int x = 0; x < num4x4W; x += stepX) {
+      int startX = baseX + 4 * x, startY = baseY + 4 * y;
+      if (startX >= ((fp->mi_cols * 4) >> sub) || startY >= ((fp->mi_rows * 4) >> sub)) continue;
+      int row = (startY << sub) >> 2, col = (startX << sub) >> 2;
+      int sbr = row & 15, sbc = col & 15;
+      if (!isInter) {
+        pred::IntraArgs a;
+        a.haveLeft = AvailL || x > 0;
+        a.haveAbove = AvailU || y > 0;
+        a.haveAboveRight = BD(sm, plane, (sbr >> sub) - 1, (sbc >> sub) + stepX);
+        a.haveBelowLeft = BD(sm, plane, (sbr >> sub) + stepY, (sbc >> sub) - 1);
+        int isCfl = plane > 0 && b.uv_mode == UV_CFL_PRED;
+        a.mode = plane == 0 ? b.y_mode : (isCfl ? DC_PRED : b.uv_mode);
+        a.angleDelta = plane == 0 ? b.angle_y : b.angle_uv;
+        a.log2W = T(Tx_Width_Log2)[txSz];
+        a.log2H = T(Tx_Height_Log2)[txSz];
+        a.maxX = ((fp->mi_cols * 4) >> sub) - 1;
+        a.maxY = ((fp->mi_rows * 4) >> sub) - 1;
+        a.edgeFilter = fp->enable_intra_edge_filter;
+        a.filterType = (b.interp_filter >> (plane == 0 ? 4 : 5)) & 1;
+        pred::IntraState st;
+        pred::intra_state(a, &st);
+        pred::intra_edges(px, stride, startX, startY, a, st, above, left, etmp, (int)threadIdx.x, RT, CtaSync());
+        int tw = 1 << a.log2W, th = 1 << a.log2H;
+        int dcv = a.mode == DC_PRED ? pred::intra_dc(a, above, left) : 0;
+        uint8_t *d = px + startY * stride + startX;
+        for (int k = threadIdx.x; k < tw * th; k += RT) {
+          int i = k >> a.log2W, j = k & (tw - 1);
+          d[i * stride + j] = (uint8_t)(a.mode == DC_PRED ? dcv : pred::intra_pixel(a, st, above, left, i, j));
+        }
+        __syncthreads();
+        if (isCfl) {
+          const uint8_t *luma = c.rec + fp->offset[0];
+          int alpha, avg;
+          if (txIdx > 0) {
+            alpha = plane == 1 ? b.cfl_alpha_u : b.cfl_alpha_v;
+            int n = tw * th;
+            long long sum = 0;
+            for (int k = threadIdx.x; k < n; k += RT)
+              sum += pred::cfl_luma(luma, fp->stride[0], startX, startY, sm.maxLumaW, sm.maxLumaH, k >> a.log2W, k & (tw - 1));
+            avg = round2((int)cta_sum64(sum, sm), a.log2W + a.log2H);
+          } else {
+            alpha = cfl_alpha(sm, luma, fp->stride[0], startX, startY, sm.maxLumaW, sm.maxLumaH, a.log2W, a.log2H, dcv,
+                              spx + startY * stride + startX, stride, plane == 2 && b.cfl_alpha_u == 0, &avg);
+            if (threadIdx.x == 0) {
+              if (plane == 1) b.cfl_alpha_u = alpha;
+              else b.cfl_alpha_v = alpha;
+            }
+          }
+          for (int k = threadIdx.x; k < tw * th; k += RT) {
+            int i = k >> a.log2W, j = k & (tw - 1);
+            int v = pred::cfl_luma(luma, fp->stride[0], startX, startY, sm.maxLumaW, sm.maxLumaH, i, j);
+            d[i * stride + j] = (uint8_t)pred::cfl_pixel(dcv, alpha, v, avg);
+          }
+          __syncthreads();
+        }
+      }
+      if (plane == 0 && threadIdx.x == 0) {
+        sm.maxLumaW = startX + stepX * 4;
+        sm.maxLumaH = startY + stepY * 4;
+      }
+      int t = DCT_DCT;
+      long long cst = 0;
+      int eob = code_tx(c, sm, spx, px, stride, startX, startY, txSz, plane, cands, numCands,
+                        c.coefs + b.coef_off[plane] + txIdx * T(Tx_Width)[txSz] * T(Tx_Height)[txSz], &t, &cst);
+      total += cst;
+      if (threadIdx.x == 0) {
+        if (plane == 0) {
+          tx_type_set(b, txIdx, t);
+          if (txIdx == 0) b.tx_type = t;
+        }
+        for (int i = 0; i < stepY; i++)
+          for (int j = 0; j < stepX; j++) BD(sm, plane, (sbr >> sub) + i, (sbc >> sub) + j) = 1;
+      }
+      txIdx++;
+      anyNz |= eob > 0;
+      __syncthreads();
+    }
+  }
+  if (threadIdx.x == 0) b.eob[plane] = anyNz;
+  __syncthreads();
+  return total;
+}
+
+// The BlockDecoded marks code_plane leaves for an inter block (phase 1).
+__device__ void mark_bd_inter(const FrameParams *fp, Smem &sm, const BlockInfo &b) {
+  if (threadIdx.x != 0) return;
+  for (int plane = 0; plane < 3; plane++) {
+    int sub = plane > 0;
+    int txSz = fp->lossless ? TX_4X4 : plane > 0 ? uv_tx_size(b.bsize, 1, 1) : T(Max_Tx_Size_Rect)[b.bsize];
+    int planeSz = T(Subsampled_Size)[b.bsize][sub][sub];
+    int num4x4W = T(Num_4x4_Blocks_Wide)[planeSz], num4x4H = T(Num_4x4_Blocks_High)[planeSz];
+    int baseX = (b.mi_col >> sub) * 4, baseY = (b.mi_row >> sub) * 4;
+    int stepX = T(Tx_Width)[txSz] >> 2, stepY = T(Tx_Height)[txSz] >> 2;
+    for (int y = 0; y < num4x4H; y += stepY)
+      for (int x = 0; x < num4x4W; x += stepX) {
+        int startX = baseX + 4 * x, startY = baseY + 4 * y;
+        if (startX >= ((fp->mi_cols * 4) >> sub) || startY >= ((fp->mi_rows * 4) >> sub)) continue;
+        int sbr = ((startY << sub) >> 2) & 15, sbc = ((startX << sub) >> 2) & 15;
+        for (int i = 0; i < stepY; i++)
+          for (int j = 0; j < stepX; j++) BD(sm, plane, (sbr >> sub) + i, (sbc >> sub) + j) = 1;
+      }
+  }
+}
+
+// One block (recon_block, k_recon.h:293-394); sm.blk holds it.
+__device__ void recon_block(const Ctx &c, Smem &sm) {
+  const FrameParams *fp = c.fp;
+  BlockInfo &b = sm.blk;
+  int bs = b.bsize;
+  int comp = b.is_inter && b.ref_frame1 > INTRA_FRAME;
+  const uint8_t *ref = (b.is_inter && b.ref_frame != LAST_FRAME) ? c.gold : c.ref;
+  const uint8_t *ref1 = c.gold;
+  int MiRow = b.mi_row, MiCol = b.mi_col;
+  if (threadIdx.x == 0) {
+    sm.maxLumaW = sm.maxLumaH = 0;
+    b.tx_depth = 0;
+    b.interp_filter &= 0x30;
+  }
+  __syncthreads();
+  int tid = threadIdx.x;
+  if (b.is_inter && fp->switchable_interp && !comp) {
+    int w = block_w(bs), h = block_h(bs);
+    int x0 = MiCol * 4, y0 = MiRow * 4, stride = fp->stride[0];
+    uint8_t *px = c.rec + fp->offset[0] + y0 * stride + x0;
+    const uint8_t *sp = c.src + fp->offset[0] + y0 * stride + x0;
+    int vw = imin(w, fp->frame_w - x0), vh = imin(h, fp->frame_h - y0);
+    long long best = -1;
+    int bestPacked = 0;
+    for (int f = 0; f < 9; f++) {
+      int packed = (f % 3) | ((f / 3) << 2);
+      pred::Inter ip;
+      pred::inter_setup(&ip, ref + fp->offset[0], stride, fp->frame_w, fp->frame_h, x0, y0, w, h, b.mv_row, b.mv_col,
+                        0, 0, packed);
+      long long sse = 0;
+      for (int k = tid; k < w * h; k += RT) {
+        int i = k / w, j = k % w;
+        int v = pred::inter_pixel(&ip, i, j);
+        px[i * stride + j] = (uint8_t)v;
+        if (i < vh && j < vw) {
+          int d = v - (int)sp[i * stride + j];
+          sse += d * d;
+        }
+      }
+      sse = cta_sum64(sse, sm);
+      long long cst = sse * 16 + (long long)fp->lambda * ((f % 3 != 0) + (f / 3 != 0));
+      if (best < 0 || cst < best) {
+        best = cst;
+        bestPacked = packed;
+      }
+    }
+    if (tid == 0) b.interp_filter = bestPacked;
+    __syncthreads();
+  }
+  for (int plane = 0; plane < 3; plane++) {
+    int sub = plane > 0, stride = fp->stride[plane];
+    int baseX = (MiCol >> sub) * 4, baseY = (MiRow >> sub) * 4;
+    if (b.is_inter) {
+      int w = block_w(bs) >> sub, h = block_h(bs) >> sub;
+      uint8_t *d = c.rec + fp->offset[plane] + baseY * stride + baseX;
+      pred::Inter p0, p1;
+      pred::inter_setup(&p0, ref + fp->offset[plane], stride, fp->frame_w, fp->frame_h, baseX, baseY, w, h, b.mv_row,
+                        b.mv_col, sub, sub, b.interp_filter);
+      if (comp)
+        pred::inter_setup(&p1, ref1 + fp->offset[plane], stride, fp->frame_w, fp->frame_h, baseX, baseY, w, h,
+                          b.mv1_row, b.mv1_col, sub, sub, b.interp_filter);
+      for (int k = tid; k < w * h; k += RT) {
+        int i = k / w, j = k % w;
+        int v = comp ? clip1(round2(pred::inter_raw(&p0, i, j) + pred::inter_raw(&p1, i, j), 5))
+                     : pred::inter_pixel(&p0, i, j);
+        d[i * stride + j] = (uint8_t)v;
+      }
+      __syncthreads();
+    }
+    if (fp->lossless) {
+      code_plane(c, sm, plane, TX_4X4);
+      continue;
+    }
+    if (plane > 0) {
+      code_plane(c, sm, plane, uv_tx_size(bs, 1, 1));
+      continue;
+    }
+    int maxDepth = (!b.is_inter && fp->tx_mode_select) ? imin(MAX_TX_DEPTH, T(Max_Tx_Depth)[bs]) : 0;
+    if (maxDepth == 0) {
+      code_plane(c, sm, 0, T(Max_Tx_Size_Rect)[bs]);
+      continue;
+    }
+    // tx_depth RD search: every depth from the same pixels and BlockDecoded
+    // flags, the winner re-coded last unless it already was
+    int w = block_w(bs), h = block_h(bs);
+    uint8_t *px = c.rec + fp->offset[0] + baseY * stride + baseX;
+    for (int k = tid; k < w * h; k += RT) sm.save[k] = px[(k / w) * stride + (k % w)];
+    for (int k = tid; k < BD_DIM * BD_DIM; k += RT) sm.bdsave[k] = sm.bd[k];
+    __syncthreads();
+    long long best = -1;
+    int bestD = 0;
+    for (int d = 0; d <= maxDepth + 1; d++) {
+      int depth = d <= maxDepth ? d : bestD;
+      if (d == maxDepth + 1 && bestD == maxDepth) break;
+      if (d > 0) {
+        for (int k = tid; k < w * h; k += RT) px[(k / w) * stride + (k % w)] = sm.save[k];
+        for (int k = tid; k < BD_DIM * BD_DIM; k += RT) sm.bd[k] = sm.bdsave[k];
+        __syncthreads();
+      }
+      long long cst = code_plane(c, sm, 0, depth_tx_size(bs, depth)) + (long long)fp->lambda * 8 * depth;
+      if (d <= maxDepth && (best < 0 || cst < best)) {
+        best = cst;
+        bestD = depth;
+      }
+      if (d == maxDepth + 1) break;
+    }
+    if (tid == 0) b.tx_depth = bestD;
+    __syncthreads();
+  }
+}
+
+// clear_block_decoded_flags( r, c, 16 ) (k_recon.h:402-414).
+__device__ void clear_bd(const FrameParams *fp, Smem &sm, int r, int c) {
+  for (int k = threadIdx.x; k < 3 * BD_DIM * BD_DIM; k += RT) sm.bd[k] = 0;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int plane = 0; plane < 3; plane++) {
+      int sub = plane > 0;
+      int sbWidth4 = (tile_col_end(fp, c) - c) >> sub;
+      int sbHeight4 = (fp->mi_rows - r) >> sub;
+      for (int y = -1; y <= (16 >> sub); y++)
+        for (int x = -1; x <= (16 >> sub); x++) {
+          if (y < 0 && x < sbWidth4) BD(sm, plane, y, x) = 1;
+          else if (x < 0 && y < sbHeight4) BD(sm, plane, y, x) = 1;
+          else BD(sm, plane, y, x) = 0;
+        }
+      BD(sm, plane, 16 >> sub, -1) = 0;
+    }
+  }
+  __syncthreads();
+}
+
+// phase 0: every inter block of superblock sbList[blockIdx.x] (or blockIdx.x);
+// phase 1: its intra blocks in decode order with BlockDecoded tracking.
+__global__ void __launch_bounds__(RT) k_recon(Ctx c, const int *sbList, int phase) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Smem &sm = *(Smem *)smem_raw;
+  const FrameParams *fp = c.fp;
+  int sb = sbList ? sbList[blockIdx.x] : blockIdx.x;
+  SbInfo sbi = c.sbs[sb];
+  if (phase == 1) {
+    if (threadIdx.x == 0) {
+      int any = 0;
+      for (int k = 0; k < sbi.num_blocks; k++) any |= !c.blocks[sbi.first_block + k].is_inter;
+      sm.flag = any;
+    }
+    __syncthreads();
+    if (!sm.flag) return;
+    clear_bd(fp, sm, sbi.sb_row * 16, sbi.sb_col * 16);
+  }
+  for (int k = 0; k < sbi.num_blocks; k++) {
+    BlockInfo *gb = &c.blocks[sbi.first_block + k];
+    if (threadIdx.x == 0) sm.blk = *gb;
+    __syncthreads();
+    int inter = sm.blk.is_inter;
+    if (phase == 0 ? inter : !inter) {
+      recon_block(c, sm);
+      if (threadIdx.x == 0) *gb = sm.blk;
+    } else if (phase == 1) {
+      mark_bd_inter(fp, sm, sm.blk);
+    }
+    __syncthreads();
+  }
+}
+
+}  // namespace rec

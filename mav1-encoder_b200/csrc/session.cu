@@ -1,0 +1,550 @@
+// libmav1cu: the C ABI of include/mav1cu.h over the sm_100a stage kernels.
+//
+// Single translation unit: the constant tables (tables.inc) and every stage
+// (me.cuh, analysis.cuh, recon.cuh, filters.cuh) are compiled here so the
+// tables exist once per device image.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdarg.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <vector>
+
+#include "common.cuh"
+#include "tables.inc"
+#include "tx.cuh"
+#include "pred.cuh"
+#include "me.cuh"
+#include "analysis.cuh"
+#include "recon.cuh"
+#include "filters.cuh"
+
+namespace {
+
+struct Geometry {
+  int w, h, mi_cols, mi_rows, sb_cols, sb_rows, num_sbs;
+  int stride[3], plane_h[3], offset[3];
+  size_t frame_bytes;
+};
+
+Geometry make_geometry(int w, int h) {
+  // frame layout of the reference encoder (encoder.c:93-120)
+  Geometry g;
+  g.w = w;
+  g.h = h;
+  g.mi_cols = 2 * ((w + 7) >> 3);
+  g.mi_rows = 2 * ((h + 7) >> 3);
+  g.sb_cols = (g.mi_cols + 15) >> 4;
+  g.sb_rows = (g.mi_rows + 15) >> 4;
+  g.num_sbs = g.sb_cols * g.sb_rows;
+  g.stride[0] = g.sb_cols * 64;
+  g.stride[1] = g.stride[2] = g.sb_cols * 32;
+  g.plane_h[0] = g.sb_rows * 64;
+  g.plane_h[1] = g.plane_h[2] = g.sb_rows * 32;
+  g.offset[0] = 0;
+  g.offset[1] = g.stride[0] * g.plane_h[0];
+  g.offset[2] = g.offset[1] + g.stride[1] * g.plane_h[1];
+  g.frame_bytes = (size_t)g.offset[2] + (size_t)g.stride[2] * g.plane_h[2];
+  return g;
+}
+
+}  // namespace
+
+struct mav1cu_session {
+  Geometry g;
+  int max_presets;
+  cudaStream_t stream, own_stream;
+  void *buf[MAV1CU_BUF_COUNT];
+  size_t size[MAV1CU_BUF_COUNT];
+  // internal device state
+  uint8_t *qp[2];          // 16 quarter-pel planes per reference
+  uint8_t *dsrc, *dref[2]; // decimated planes
+  uint8_t *ys, *uvs;       // edge-type marks per mi
+  int *waves;              // superblock lists of the intra waves
+  int *status;             // device status word
+  std::vector<int> wave_start, wave_len;
+  int wave_tile_w;
+  FrameParams fp;          // host copy of the current parameters
+  int have_params;
+  int64_t launches;
+  int err;
+  char msg[512];
+};
+
+static int set_error(mav1cu_session *s, int code, const char *fmt, ...) {
+  if (!s->err) {
+    s->err = code;
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(s->msg, sizeof s->msg, fmt, ap);
+    va_end(ap);
+  }
+  return s->err;
+}
+
+static int check_cuda(mav1cu_session *s, cudaError_t e, const char *what) {
+  if (e != cudaSuccess) return set_error(s, MAV1CU_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+  return MAV1CU_OK;
+}
+
+static int after_launch(mav1cu_session *s, const char *what) {
+  s->launches++;
+  return check_cuda(s, cudaGetLastError(), what);
+}
+
+// ---- inverse scan tables ------------------------------------------------------------
+
+// Scan table of (txSz, type) exactly as the reference selects it (get_scan
+// and its per-size fallbacks, k_scan.h:241-292).
+static const int32_t *host_scan(int txSz, int t, int *len) {
+  if (txSz == TX_16X64) { *len = 512; return h_Default_Scan_16x32; }
+  if (txSz == TX_64X16) { *len = 512; return h_Default_Scan_32x16; }
+  if (h_Tx_Size_Sqr_Up[txSz] == TX_64X64) { *len = 1024; return h_Default_Scan_32x32; }
+  int preferRow = t == V_DCT || t == V_ADST || t == V_FLIPADST;
+  int preferCol = t == H_DCT || t == H_ADST || t == H_FLIPADST;
+  if (t == IDTX) preferRow = preferCol = 0;
+#define SZ(tx, name, n) if (txSz == tx) { *len = n; return h_##name; }
+  if (preferRow) {
+    SZ(TX_4X4, Mrow_Scan_4x4, 16) SZ(TX_4X8, Mrow_Scan_4x8, 32) SZ(TX_8X4, Mrow_Scan_8x4, 32)
+    SZ(TX_8X8, Mrow_Scan_8x8, 64) SZ(TX_8X16, Mrow_Scan_8x16, 128) SZ(TX_16X8, Mrow_Scan_16x8, 128)
+    SZ(TX_16X16, Mrow_Scan_16x16, 256) SZ(TX_4X16, Mrow_Scan_4x16, 64)
+    *len = 64;
+    return h_Mrow_Scan_16x4;
+  }
+  if (preferCol) {
+    SZ(TX_4X4, Mcol_Scan_4x4, 16) SZ(TX_4X8, Mcol_Scan_4x8, 32) SZ(TX_8X4, Mcol_Scan_8x4, 32)
+    SZ(TX_8X8, Mcol_Scan_8x8, 64) SZ(TX_8X16, Mcol_Scan_8x16, 128) SZ(TX_16X8, Mcol_Scan_16x8, 128)
+    SZ(TX_16X16, Mcol_Scan_16x16, 256) SZ(TX_4X16, Mcol_Scan_4x16, 64)
+    *len = 64;
+    return h_Mcol_Scan_16x4;
+  }
+  SZ(TX_4X4, Default_Scan_4x4, 16) SZ(TX_4X8, Default_Scan_4x8, 32) SZ(TX_8X4, Default_Scan_8x4, 32)
+  SZ(TX_8X8, Default_Scan_8x8, 64) SZ(TX_8X16, Default_Scan_8x16, 128) SZ(TX_16X8, Default_Scan_16x8, 128)
+  SZ(TX_16X16, Default_Scan_16x16, 256) SZ(TX_16X32, Default_Scan_16x32, 512)
+  SZ(TX_32X16, Default_Scan_32x16, 512) SZ(TX_4X16, Default_Scan_4x16, 64) SZ(TX_16X4, Default_Scan_16x4, 64)
+  SZ(TX_8X32, Default_Scan_8x32, 256) SZ(TX_32X8, Default_Scan_32x8, 256)
+#undef SZ
+  *len = 1024;
+  return h_Default_Scan_32x32;
+}
+
+static int upload_inverse_scans(mav1cu_session *s) {
+  static const int rep[3] = {DCT_DCT, V_DCT, H_DCT};
+  std::vector<int16_t> data;
+  std::vector<const int32_t *> seen;
+  std::vector<int> seenOff;
+  int off[3][19];
+  for (int k = 0; k < 3; k++)
+    for (int t = 0; t < 19; t++) {
+      int len;
+      const int32_t *sc = host_scan(t, rep[k], &len);
+      int found = -1;
+      for (size_t i = 0; i < seen.size(); i++)
+        if (seen[i] == sc) found = seenOff[i];
+      if (found < 0) {
+        found = (int)data.size();
+        seen.push_back(sc);
+        seenOff.push_back(found);
+        data.resize(data.size() + len);
+        for (int c = 0; c < len; c++) data[found + sc[c]] = (int16_t)c;
+      }
+      off[k][t] = found;
+    }
+  if (data.size() > 8192) return set_error(s, MAV1CU_ERR_ARG, "inverse scan tables exceed their space");
+  if (check_cuda(s, cudaMemcpyToSymbol(rec::d_inv_scan, data.data(), data.size() * sizeof(int16_t)), "scan tables"))
+    return s->err;
+  return check_cuda(s, cudaMemcpyToSymbol(rec::d_inv_scan_off, off, sizeof off), "scan offsets");
+}
+
+// ---- forward matrices (fwd_matrices.c:17-65) ---------------------------------------------
+
+// Matrix of the 1-D inverse kernel `kind` of length n applied to scaled
+// impulses, then its least-squares inverse F = (A^T A)^-1 A^T by Gauss-Jordan
+// with partial pivoting, rounded to Q20. The double-precision operations and
+// their order are those of the reference derivation, so the integer tables
+// are identical (checked against the reference's table by the tests).
+static void build_fwd_one(int kind, int log2n, int32_t *out) {
+  int n = 1 << log2n, m = n > 32 ? 32 : n;
+  static double A[64][32], M[32][32 + 64];
+  const double S = 65536.0;
+  for (int j = 0; j < m; j++) {
+    int32_t t[64];
+    for (int i = 0; i < 64; i++) t[i] = 0;
+    t[j] = (int32_t)S;
+    tx::inverse_1d(t, kind, log2n, 31);
+    for (int i = 0; i < n; i++) A[i][j] = t[i] / S;
+  }
+  for (int r = 0; r < m; r++) {
+    for (int c = 0; c < m; c++) {
+      double acc = 0;
+      for (int i = 0; i < n; i++) acc += A[i][r] * A[i][c];
+      M[r][c] = acc;
+    }
+    for (int i = 0; i < n; i++) M[r][m + i] = A[i][r];
+  }
+  for (int p = 0; p < m; p++) {
+    int best = p;
+    for (int r = p + 1; r < m; r++)
+      if (fabs(M[r][p]) > fabs(M[best][p])) best = r;
+    if (best != p)
+      for (int c = 0; c < m + n; c++) {
+        double t = M[p][c];
+        M[p][c] = M[best][c];
+        M[best][c] = t;
+      }
+    double inv = 1.0 / M[p][p];
+    for (int c = 0; c < m + n; c++) M[p][c] *= inv;
+    for (int r = 0; r < m; r++) {
+      if (r == p || M[r][p] == 0) continue;
+      double f = M[r][p];
+      for (int c = 0; c < m + n; c++) M[r][c] -= f * M[p][c];
+    }
+  }
+  for (int k = 0; k < m; k++)
+    for (int i = 0; i < n; i++) out[k * n + i] = (int32_t)lrint(M[k][m + i] * (double)(1 << 20));
+}
+
+extern "C" void mav1cu_build_fwd_matrices(int32_t *mats) {
+  memset(mats, 0, sizeof(int32_t) * 4096 * 15);
+  for (int kind = 0; kind < 3; kind++)
+    for (int log2n = 2; log2n <= 6; log2n++) {
+      if (kind == tx::KIND_ADST && log2n > 4) continue;
+      if (kind == tx::KIND_IDTX && log2n > 5) continue;
+      build_fwd_one(kind, log2n, mats + rec::fwd_slot(kind, log2n));
+    }
+}
+
+// ---- session -------------------------------------------------------------------------
+
+static void free_all(mav1cu_session *s) {
+  for (int i = 0; i < MAV1CU_BUF_COUNT; i++)
+    if (s->buf[i]) cudaFree(s->buf[i]);
+  void *extra[] = {s->qp[0], s->qp[1], s->dsrc, s->dref[0], s->dref[1], s->ys, s->uvs, s->waves, s->status};
+  for (void *p : extra)
+    if (p) cudaFree(p);
+  if (s->own_stream) cudaStreamDestroy(s->own_stream);
+}
+
+extern "C" int mav1cu_session_create(int width, int height, int max_cdef_presets, mav1cu_session **out, char *err,
+                                     size_t errlen) {
+  *out = NULL;
+  if (width < 16 || height < 16 || width > 65536 || height > 65536 || max_cdef_presets < 0 || max_cdef_presets > 4) {
+    snprintf(err, errlen, "unsupported session %dx%d (%d CDEF presets)", width, height, max_cdef_presets);
+    return MAV1CU_ERR_ARG;
+  }
+  mav1cu_session *s = new mav1cu_session();
+  s->g = make_geometry(width, height);
+  s->max_presets = max_cdef_presets;
+  const Geometry &g = s->g;
+  size_t fb = g.frame_bytes, nsb = (size_t)g.num_sbs;
+  s->size[MAV1CU_BUF_SRC] = s->size[MAV1CU_BUF_REC] = s->size[MAV1CU_BUF_REF] = s->size[MAV1CU_BUF_GOLD] = fb;
+  s->size[MAV1CU_BUF_DBK] = s->size[MAV1CU_BUF_LROUT] = fb;
+  s->size[MAV1CU_BUF_PARAMS] = sizeof(FrameParams);
+  s->size[MAV1CU_BUF_MATS] = sizeof(int32_t) * 4096 * 15;
+  s->size[MAV1CU_BUF_MVFIELD] = s->size[MAV1CU_BUF_MVGOLD] = sizeof(int32_t) * 2 * NUM_NODES * nsb;
+  s->size[MAV1CU_BUF_BLOCKS] = sizeof(BlockInfo) * MAX_BLOCKS_PER_SB * nsb;
+  s->size[MAV1CU_BUF_SBS] = sizeof(SbInfo) * nsb;
+  s->size[MAV1CU_BUF_COEFS] = sizeof(int32_t) * COEFS_PER_SB * nsb;
+  s->size[MAV1CU_BUF_LFMASK] = (size_t)g.mi_rows * g.mi_cols;
+  s->size[MAV1CU_BUF_CDEFBUF] = fb * (max_cdef_presets ? max_cdef_presets : 1);
+  s->size[MAV1CU_BUF_CDEF_CHOICE] = nsb;
+  s->size[MAV1CU_BUF_LRUNITS] = sizeof(LrUnit) * 3 * (size_t)(g.sb_rows + 1) * (g.sb_cols + 1);
+  s->size[MAV1CU_BUF_ACOSTS] = sizeof(int64_t) * A_ITEMS * nsb;
+  s->size[MAV1CU_BUF_AINFOS] = sizeof(BlockInfo) * A_ITEMS * nsb;
+  cudaError_t e = cudaSuccess;
+  for (int i = 0; i < MAV1CU_BUF_COUNT && e == cudaSuccess; i++) {
+    e = cudaMalloc(&s->buf[i], s->size[i]);
+    if (e == cudaSuccess) e = cudaMemset(s->buf[i], 0, s->size[i]);
+  }
+  size_t plane = (size_t)width * height, dplane = (size_t)((width + 3) >> 2) * ((height + 3) >> 2);
+  if (e == cudaSuccess) e = cudaMalloc(&s->qp[0], 16 * plane);
+  if (e == cudaSuccess) e = cudaMalloc(&s->qp[1], 16 * plane);
+  if (e == cudaSuccess) e = cudaMalloc(&s->dsrc, dplane);
+  if (e == cudaSuccess) e = cudaMalloc(&s->dref[0], dplane);
+  if (e == cudaSuccess) e = cudaMalloc(&s->dref[1], dplane);
+  if (e == cudaSuccess) e = cudaMalloc(&s->ys, (size_t)g.mi_rows * g.mi_cols);
+  if (e == cudaSuccess) e = cudaMalloc(&s->uvs, (size_t)g.mi_rows * g.mi_cols);
+  if (e == cudaSuccess) e = cudaMalloc(&s->waves, sizeof(int) * nsb);
+  if (e == cudaSuccess) e = cudaMalloc(&s->status, sizeof(int) * 4);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->own_stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    snprintf(err, errlen, "device allocation failed: %s", cudaGetErrorString(e));
+    free_all(s);
+    delete s;
+    return e == cudaErrorMemoryAllocation ? MAV1CU_ERR_NOMEM : MAV1CU_ERR_CUDA;
+  }
+  s->stream = s->own_stream;
+  cudaMemset(s->status, 0, sizeof(int) * 4);
+  std::vector<int32_t> mats(4096 * 15);
+  mav1cu_build_fwd_matrices(mats.data());
+  cudaMemcpy(s->buf[MAV1CU_BUF_MATS], mats.data(), mats.size() * sizeof(int32_t), cudaMemcpyHostToDevice);
+  if (upload_inverse_scans(s) || check_cuda(s, cudaDeviceSynchronize(), "session setup")) {
+    snprintf(err, errlen, "%s", s->msg);
+    int code = s->err;
+    mav1cu_session_destroy(s);
+    return code;
+  }
+  cudaFuncSetAttribute(rec::k_recon, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(rec::Smem));
+  cudaFuncSetAttribute(ana::k_analyze_level, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)(4 * sizeof(ana::WarpMem)));
+  *out = s;
+  return MAV1CU_OK;
+}
+
+extern "C" void mav1cu_session_destroy(mav1cu_session *s) {
+  if (!s) return;
+  cudaStreamSynchronize(s->stream);
+  free_all(s);
+  delete s;
+}
+
+extern "C" int mav1cu_set_stream(mav1cu_session *s, void *stream) {
+  s->stream = stream ? (cudaStream_t)stream : s->own_stream;
+  return MAV1CU_OK;
+}
+extern "C" void *mav1cu_get_stream(mav1cu_session *s) { return (void *)s->stream; }
+
+extern "C" size_t mav1cu_buf_size(const mav1cu_session *s, int buf) {
+  return buf >= 0 && buf < MAV1CU_BUF_COUNT ? s->size[buf] : 0;
+}
+extern "C" void *mav1cu_buf_device(mav1cu_session *s, int buf) {
+  return buf >= 0 && buf < MAV1CU_BUF_COUNT ? s->buf[buf] : NULL;
+}
+
+extern "C" int mav1cu_upload(mav1cu_session *s, int buf, const void *host, size_t bytes) {
+  if (s->err) return s->err;
+  if (buf < 0 || buf >= MAV1CU_BUF_COUNT || bytes > s->size[buf])
+    return set_error(s, MAV1CU_ERR_ARG, "upload: buffer %d, %zu bytes", buf, bytes);
+  return check_cuda(s, cudaMemcpyAsync(s->buf[buf], host, bytes, cudaMemcpyHostToDevice, s->stream), "upload");
+}
+
+extern "C" int mav1cu_download(mav1cu_session *s, int buf, void *host, size_t bytes) {
+  if (s->err) return s->err;
+  if (buf < 0 || buf >= MAV1CU_BUF_COUNT || bytes > s->size[buf])
+    return set_error(s, MAV1CU_ERR_ARG, "download: buffer %d, %zu bytes", buf, bytes);
+  return check_cuda(s, cudaMemcpyAsync(host, s->buf[buf], bytes, cudaMemcpyDeviceToHost, s->stream), "download");
+}
+
+extern "C" int mav1cu_copy(mav1cu_session *s, int dst, int src, size_t bytes) {
+  if (s->err) return s->err;
+  if (dst < 0 || dst >= MAV1CU_BUF_COUNT || src < 0 || src >= MAV1CU_BUF_COUNT || bytes > s->size[dst] ||
+      bytes > s->size[src])
+    return set_error(s, MAV1CU_ERR_ARG, "copy: buffers %d <- %d, %zu bytes", dst, src, bytes);
+  return check_cuda(s, cudaMemcpyAsync(s->buf[dst], s->buf[src], bytes, cudaMemcpyDeviceToDevice, s->stream), "copy");
+}
+
+// Superblock lists of the intra waves: wave (c - tileStart) + 2r holds the
+// superblocks whose left and above-right neighbours are in earlier waves.
+static int build_waves(mav1cu_session *s, int tile_w_sb) {
+  const Geometry &g = s->g;
+  int nw = tile_w_sb + 2 * (g.sb_rows - 1);
+  std::vector<int> list;
+  s->wave_start.assign(nw, 0);
+  s->wave_len.assign(nw, 0);
+  for (int w = 0; w < nw; w++) {
+    s->wave_start[w] = (int)list.size();
+    for (int r = 0; r < g.sb_rows; r++)
+      for (int c = 0; c < g.sb_cols; c++)
+        if ((c % tile_w_sb) + 2 * r == w) list.push_back(r * g.sb_cols + c);
+    s->wave_len[w] = (int)list.size() - s->wave_start[w];
+  }
+  s->wave_tile_w = tile_w_sb;
+  return check_cuda(s, cudaMemcpy(s->waves, list.data(), list.size() * sizeof(int), cudaMemcpyHostToDevice), "waves");
+}
+
+extern "C" int mav1cu_set_params(mav1cu_session *s, const mav1cu_frame_params *fp) {
+  if (s->err) return s->err;
+  const Geometry &g = s->g;
+  if (fp->mi_cols != g.mi_cols || fp->mi_rows != g.mi_rows || fp->frame_w != g.w || fp->frame_h != g.h ||
+      fp->stride[0] != g.stride[0] || fp->offset[1] != g.offset[1] || fp->tile_w_sb < 1)
+    return set_error(s, MAV1CU_ERR_ARG, "frame parameters do not match the session geometry");
+  s->fp = *fp;
+  s->have_params = 1;
+  if (s->wave_tile_w != fp->tile_w_sb && build_waves(s, fp->tile_w_sb)) return s->err;
+  return mav1cu_upload(s, MAV1CU_BUF_PARAMS, fp, sizeof(FrameParams));
+}
+
+static int need_params(mav1cu_session *s) {
+  if (s->err) return s->err;
+  if (!s->have_params) return set_error(s, MAV1CU_ERR_ARG, "stage called before mav1cu_set_params");
+  return MAV1CU_OK;
+}
+
+#define DP(s) ((const FrameParams *)(s)->buf[MAV1CU_BUF_PARAMS])
+#define U8(s, b) ((uint8_t *)(s)->buf[b])
+
+extern "C" int mav1cu_motion_search(mav1cu_session *s) {
+  if (need_params(s)) return s->err;
+  const FrameParams &fp = s->fp;
+  int nref = fp.golden ? 2 : 1;
+  const uint8_t *refs[2] = {U8(s, MAV1CU_BUF_REF), U8(s, MAV1CU_BUF_GOLD)};
+  if (fp.turbo & T_ME_HPEL) {
+    dim3 blk(128), grid((fp.frame_w + 127) / 128, fp.frame_h);
+    for (int r = 0; r < nref; r++) {
+      me::k_qpel_planes<<<grid, blk, 0, s->stream>>>(DP(s), refs[r], s->qp[r]);
+      if (after_launch(s, "qpel planes")) return s->err;
+    }
+    if (fp.turbo & T_ME_DEC) {
+      int dw = (fp.frame_w + 3) >> 2, dh = (fp.frame_h + 3) >> 2;
+      dim3 dg((dw + 127) / 128, dh);
+      me::k_dec_plane<<<dg, blk, 0, s->stream>>>(DP(s), U8(s, MAV1CU_BUF_SRC), s->dsrc);
+      if (after_launch(s, "decimated source")) return s->err;
+      for (int r = 0; r < nref; r++) {
+        me::k_dec_plane<<<dg, blk, 0, s->stream>>>(DP(s), refs[r], s->dref[r]);
+        if (after_launch(s, "decimated reference")) return s->err;
+      }
+    }
+  }
+  me::Frame f[2];
+  for (int r = 0; r < 2; r++) {
+    f[r].fp = DP(s);
+    f[r].src = U8(s, MAV1CU_BUF_SRC);
+    f[r].ref = refs[r];
+    f[r].qp = s->qp[r];
+    f[r].dsrc = s->dsrc;
+    f[r].dref = s->dref[r];
+    f[r].mv = (int32_t *)s->buf[r ? MAV1CU_BUF_MVGOLD : MAV1CU_BUF_MVFIELD];
+    f[r].isGold = r;
+  }
+  for (int level = 0; level < 4; level++) {
+    int nodes = s->g.num_sbs << (2 * level);
+    dim3 grid((nodes + 3) / 4, nref);
+    me::k_me_level<<<grid, 128, 0, s->stream>>>(f[0], f[1], level);
+    if (after_launch(s, "motion search")) return s->err;
+  }
+  return MAV1CU_OK;
+}
+
+static ana::Ctx ana_ctx(mav1cu_session *s) {
+  ana::Ctx c;
+  c.fp = DP(s);
+  c.src = U8(s, MAV1CU_BUF_SRC);
+  c.ref = U8(s, MAV1CU_BUF_REF);
+  c.gold = U8(s, MAV1CU_BUF_GOLD);
+  c.mv = (const int32_t *)s->buf[MAV1CU_BUF_MVFIELD];
+  c.mvg = (const int32_t *)s->buf[MAV1CU_BUF_MVGOLD];
+  c.costs = (int64_t *)s->buf[MAV1CU_BUF_ACOSTS];
+  c.infos = (BlockInfo *)s->buf[MAV1CU_BUF_AINFOS];
+  c.blocks = (BlockInfo *)s->buf[MAV1CU_BUF_BLOCKS];
+  c.sbs = (SbInfo *)s->buf[MAV1CU_BUF_SBS];
+  return c;
+}
+
+extern "C" int mav1cu_analyze(mav1cu_session *s) {
+  if (need_params(s)) return s->err;
+  ana::Ctx c = ana_ctx(s);
+  for (int level = 0; level < 4; level++) {
+    int slots = ana::level_slots(&s->fp, level);
+    long long items = (long long)s->g.num_sbs * (1 << (2 * level)) * slots;
+    ana::k_analyze_level<<<(unsigned)((items + 3) / 4), 128, 4 * sizeof(ana::WarpMem), s->stream>>>(c, level, slots);
+    if (after_launch(s, "analysis pass 1")) return s->err;
+  }
+  ana::k_analyze_table<<<(s->g.num_sbs + 63) / 64, 64, 0, s->stream>>>(c);
+  return after_launch(s, "analysis pass 2");
+}
+
+extern "C" int mav1cu_edge_types(mav1cu_session *s) {
+  if (need_params(s)) return s->err;
+  BlockInfo *blocks = (BlockInfo *)s->buf[MAV1CU_BUF_BLOCKS];
+  const SbInfo *sbs = (const SbInfo *)s->buf[MAV1CU_BUF_SBS];
+  ana::k_edge_marks<<<s->g.num_sbs, 64, 0, s->stream>>>(DP(s), blocks, sbs, s->ys, s->uvs);
+  if (after_launch(s, "edge marks")) return s->err;
+  ana::k_edge_types<<<s->g.num_sbs, 64, 0, s->stream>>>(DP(s), blocks, sbs, s->ys, s->uvs);
+  return after_launch(s, "edge types");
+}
+
+extern "C" int mav1cu_recon(mav1cu_session *s) {
+  if (need_params(s)) return s->err;
+  rec::Ctx c;
+  c.fp = DP(s);
+  c.src = U8(s, MAV1CU_BUF_SRC);
+  c.rec = U8(s, MAV1CU_BUF_REC);
+  c.ref = U8(s, MAV1CU_BUF_REF);
+  c.gold = U8(s, MAV1CU_BUF_GOLD);
+  c.blocks = (BlockInfo *)s->buf[MAV1CU_BUF_BLOCKS];
+  c.sbs = (const SbInfo *)s->buf[MAV1CU_BUF_SBS];
+  c.coefs = (int32_t *)s->buf[MAV1CU_BUF_COEFS];
+  c.mats = (const int32_t *)s->buf[MAV1CU_BUF_MATS];
+  c.status = s->status;
+  size_t smem = sizeof(rec::Smem);
+  if (!s->fp.frame_is_intra) {
+    rec::k_recon<<<s->g.num_sbs, RT, smem, s->stream>>>(c, NULL, 0);
+    if (after_launch(s, "recon inter blocks")) return s->err;
+  }
+  // leaf frames code inter blocks only (the analysis never keeps intra there)
+  if (s->fp.leaf && !s->fp.frame_is_intra) return MAV1CU_OK;
+  for (size_t w = 0; w < s->wave_len.size(); w++) {
+    if (!s->wave_len[w]) continue;
+    rec::k_recon<<<s->wave_len[w], RT, smem, s->stream>>>(c, s->waves + s->wave_start[w], 1);
+    if (after_launch(s, "recon intra wave")) return s->err;
+  }
+  return MAV1CU_OK;
+}
+
+extern "C" int mav1cu_frame_core(mav1cu_session *s) {
+  if (need_params(s)) return s->err;
+  if (!s->fp.frame_is_intra && mav1cu_motion_search(s)) return s->err;
+  if (mav1cu_analyze(s)) return s->err;
+  if (s->fp.enable_intra_edge_filter && mav1cu_edge_types(s)) return s->err;
+  return mav1cu_recon(s);
+}
+
+extern "C" int mav1cu_filter_info(mav1cu_session *s) {
+  if (need_params(s)) return s->err;
+  flt::k_filter_info<<<s->g.num_sbs, 64, 0, s->stream>>>(DP(s), (const BlockInfo *)s->buf[MAV1CU_BUF_BLOCKS],
+                                                           (const SbInfo *)s->buf[MAV1CU_BUF_SBS],
+                                                           U8(s, MAV1CU_BUF_LFMASK));
+  return after_launch(s, "filter info");
+}
+
+extern "C" int mav1cu_filter(mav1cu_session *s, int num_cdef_presets) {
+  if (need_params(s)) return s->err;
+  if (num_cdef_presets < 0 || num_cdef_presets > s->max_presets)
+    return set_error(s, MAV1CU_ERR_ARG, "filter: %d CDEF presets (session holds %d)", num_cdef_presets, s->max_presets);
+  const FrameParams &fp = s->fp;
+  if (fp.lf_level[0] || fp.lf_level[1] || fp.lf_level[2] || fp.lf_level[3]) {
+    for (int pass = 0; pass < 2; pass++) {
+      long long lines = pass == 0 ? fp.mi_rows : fp.mi_cols, n = pass == 0 ? fp.mi_cols : fp.mi_rows;
+      long long threads = 3 * lines * n * 4;
+      flt::k_deblock<<<(unsigned)((threads + 255) / 256), 256, 0, s->stream>>>(DP(s), U8(s, MAV1CU_BUF_REC),
+                                                                               U8(s, MAV1CU_BUF_LFMASK), pass);
+      if (after_launch(s, "deblock")) return s->err;
+    }
+  }
+  if (num_cdef_presets > 0) {
+    int blocks = ((fp.mi_cols + 1) >> 1) * ((fp.mi_rows + 1) >> 1);
+    flt::k_cdef<<<blocks, 64, 0, s->stream>>>(DP(s), U8(s, MAV1CU_BUF_REC), U8(s, MAV1CU_BUF_CDEFBUF),
+                                               (long long)s->g.frame_bytes, U8(s, MAV1CU_BUF_LFMASK), num_cdef_presets);
+    if (after_launch(s, "cdef")) return s->err;
+  }
+  return MAV1CU_OK;
+}
+
+extern "C" int mav1cu_cdef_select(mav1cu_session *s, int num_cdef_presets) {
+  if (need_params(s)) return s->err;
+  if (num_cdef_presets < 1 || num_cdef_presets > s->max_presets)
+    return set_error(s, MAV1CU_ERR_ARG, "cdef_select: %d presets (session holds %d)", num_cdef_presets, s->max_presets);
+  flt::k_cdef_select<<<s->g.num_sbs, 256, 0, s->stream>>>(DP(s), U8(s, MAV1CU_BUF_SRC), U8(s, MAV1CU_BUF_CDEFBUF),
+                                                           (long long)s->g.frame_bytes, U8(s, MAV1CU_BUF_REC),
+                                                           (int8_t *)s->buf[MAV1CU_BUF_CDEF_CHOICE], num_cdef_presets);
+  return after_launch(s, "cdef select");
+}
+
+extern "C" int mav1cu_restore(mav1cu_session *s) {
+  if (need_params(s)) return s->err;
+  int n = 3 * ((s->fp.frame_h + 3) >> 2) * ((s->fp.frame_w + 3) >> 2);
+  flt::k_lr_apply<<<(n + 127) / 128, 128, 0, s->stream>>>(DP(s), U8(s, MAV1CU_BUF_REC), U8(s, MAV1CU_BUF_DBK),
+                                                           U8(s, MAV1CU_BUF_LROUT),
+                                                           (const LrUnit *)s->buf[MAV1CU_BUF_LRUNITS]);
+  return after_launch(s, "loop restoration");
+}
+
+extern "C" int mav1cu_synchronize(mav1cu_session *s) {
+  if (s->err) return s->err;
+  return check_cuda(s, cudaStreamSynchronize(s->stream), "synchronize");
+}
+
+extern "C" const char *mav1cu_error_string(const mav1cu_session *s) { return s->err ? s->msg : ""; }
+extern "C" int64_t mav1cu_launch_count(const mav1cu_session *s) { return s->launches; }

@@ -1,0 +1,218 @@
+"""Python binding of libmav1cu (include/mav1cu.h) over ctypes.
+
+This is the host-side mirror of the encoder's backend interface for tests,
+benchmarks and the batching / serving layers: a Session owns one encoder
+instance's device state; its methods are the C ABI's stage calls. Record
+formats (FrameParams, BlockInfo, SbInfo, LrUnit) are exposed as numpy dtypes
+with the reference encoder's byte layout.
+
+The CUDA library is required: importing this module on a machine where
+libmav1cu.so is absent or cannot be loaded raises, there is no CPU fallback.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libmav1cu.so")
+
+# buffer ids (include/mav1cu.h)
+BUF = dict(
+    SRC=0, REC=1, REF=2, GOLD=3, PARAMS=4, MATS=5, MVFIELD=6, MVGOLD=7, BLOCKS=8, SBS=9, COEFS=10, LFMASK=11,
+    CDEFBUF=12, CDEF_CHOICE=13, DBK=14, LROUT=15, LRUNITS=16, ACOSTS=17, AINFOS=18,
+)
+
+PARAM_FIELDS = [
+    ("mi_cols", 1), ("mi_rows", 1), ("sb_cols", 1), ("sb_rows", 1), ("plane_w", 3), ("plane_h", 3), ("stride", 3),
+    ("offset", 3), ("base_q_idx", 1), ("dc_q", 3), ("ac_q", 3), ("frame_is_intra", 1), ("reduced_tx_set", 1),
+    ("enable_intra_edge_filter", 1), ("tx_search", 1), ("lambda", 1), ("wave", 1), ("num_blocks", 1),
+    ("frame_w", 1), ("frame_h", 1), ("me_range", 1), ("lossless", 1), ("tx_mode_select", 1), ("tile_w_sb", 1),
+    ("fast", 1), ("leaf", 1), ("depth_thr", 1), ("switchable_interp", 1), ("golden", 1), ("ref2_frame", 1),
+    ("compound", 1), ("lf_level", 4), ("lf_sharpness", 1), ("cdef_damping", 1), ("cdef_bits", 1),
+    ("cdef_y_pri", 8), ("cdef_y_sec", 8), ("cdef_uv_pri", 8), ("cdef_uv_sec", 8), ("lr_type", 3),
+    ("lr_unit_size", 3), ("lr_unit_rows", 3), ("lr_unit_cols", 3), ("lr_unit_off", 3), ("turbo", 1),
+]
+PARAMS_DTYPE = np.dtype([(n, "<i4", (k,)) if k > 1 else (n, "<i4") for n, k in PARAM_FIELDS])
+BLOCK_DTYPE = np.dtype([
+    ("mi_row", "<i4"), ("mi_col", "<i4"), ("bsize", "<i4"), ("is_inter", "<i4"), ("y_mode", "<i4"),
+    ("uv_mode", "<i4"), ("angle_y", "<i4"), ("angle_uv", "<i4"), ("mv_row", "<i4"), ("mv_col", "<i4"),
+    ("tx_type", "<i4"), ("eob", "<i4", (3,)), ("coef_off", "<i4", (3,)), ("cfl_alpha_u", "<i4"),
+    ("cfl_alpha_v", "<i4"), ("tx_depth", "<i4"), ("tx_types_lo", "<i4"), ("tx_types_hi", "<i4"),
+    ("interp_filter", "<i4"), ("ref_frame", "<i4"), ("ref_frame1", "<i4"), ("mv1_row", "<i4"), ("mv1_col", "<i4"),
+])
+SB_DTYPE = np.dtype([("first_block", "<i4"), ("num_blocks", "<i4"), ("sb_row", "<i4"), ("sb_col", "<i4"),
+                     ("part", "<i4", (85,))])
+LRUNIT_DTYPE = np.dtype([("type", "<i4"), ("set", "<i4"), ("xqd", "<i4", (2,)), ("wiener", "<i4", (2, 3)),
+                         ("pad", "<i4", (2,))])
+assert PARAMS_DTYPE.itemsize == 392 and BLOCK_DTYPE.itemsize == 108
+assert SB_DTYPE.itemsize == 356 and LRUNIT_DTYPE.itemsize == 48
+
+EXPORTS = [
+    "mav1cu_session_create", "mav1cu_session_destroy", "mav1cu_set_stream", "mav1cu_get_stream", "mav1cu_buf_size",
+    "mav1cu_buf_device", "mav1cu_upload", "mav1cu_download", "mav1cu_copy", "mav1cu_set_params",
+    "mav1cu_motion_search", "mav1cu_analyze", "mav1cu_edge_types", "mav1cu_recon", "mav1cu_frame_core",
+    "mav1cu_filter_info", "mav1cu_filter", "mav1cu_cdef_select", "mav1cu_restore", "mav1cu_synchronize",
+    "mav1cu_error_string", "mav1cu_launch_count", "mav1cu_build_fwd_matrices",
+]
+
+
+def load_library(path=LIB_PATH):
+    """Loads libmav1cu.so and declares its signatures; raises if missing."""
+    if not os.path.exists(path):
+        raise RuntimeError(f"libmav1cu.so not built at {path}: run __graft_entry__.build()")
+    lib = ctypes.CDLL(path)
+    vp, sz, i32 = ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int
+    lib.mav1cu_session_create.argtypes = [i32, i32, i32, ctypes.POINTER(vp), ctypes.c_char_p, sz]
+    lib.mav1cu_session_create.restype = i32
+    lib.mav1cu_session_destroy.argtypes = [vp]
+    lib.mav1cu_session_destroy.restype = None
+    lib.mav1cu_set_stream.argtypes = [vp, vp]
+    lib.mav1cu_get_stream.argtypes = [vp]
+    lib.mav1cu_get_stream.restype = vp
+    lib.mav1cu_buf_size.argtypes = [vp, i32]
+    lib.mav1cu_buf_size.restype = sz
+    lib.mav1cu_buf_device.argtypes = [vp, i32]
+    lib.mav1cu_buf_device.restype = vp
+    for f in ("mav1cu_upload", "mav1cu_download"):
+        getattr(lib, f).argtypes = [vp, i32, vp, sz]
+        getattr(lib, f).restype = i32
+    lib.mav1cu_copy.argtypes = [vp, i32, i32, sz]
+    lib.mav1cu_set_params.argtypes = [vp, vp]
+    for f in ("mav1cu_motion_search", "mav1cu_analyze", "mav1cu_edge_types", "mav1cu_recon", "mav1cu_frame_core",
+              "mav1cu_filter_info", "mav1cu_restore", "mav1cu_synchronize"):
+        getattr(lib, f).argtypes = [vp]
+        getattr(lib, f).restype = i32
+    lib.mav1cu_filter.argtypes = [vp, i32]
+    lib.mav1cu_cdef_select.argtypes = [vp, i32]
+    lib.mav1cu_error_string.argtypes = [vp]
+    lib.mav1cu_error_string.restype = ctypes.c_char_p
+    lib.mav1cu_launch_count.argtypes = [vp]
+    lib.mav1cu_launch_count.restype = ctypes.c_int64
+    lib.mav1cu_build_fwd_matrices.argtypes = [vp]
+    lib.mav1cu_build_fwd_matrices.restype = None
+    return lib
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        _lib = load_library()
+    return _lib
+
+
+class Mav1cuError(RuntimeError):
+    pass
+
+
+def geometry(width, height):
+    """Frame layout of the reference encoder (encoder.c:93-120)."""
+    mi_cols, mi_rows = 2 * ((width + 7) >> 3), 2 * ((height + 7) >> 3)
+    sb_cols, sb_rows = (mi_cols + 15) >> 4, (mi_rows + 15) >> 4
+    stride = [sb_cols * 64, sb_cols * 32, sb_cols * 32]
+    plane_h = [sb_rows * 64, sb_rows * 32, sb_rows * 32]
+    offset = [0, stride[0] * plane_h[0], stride[0] * plane_h[0] + stride[1] * plane_h[1]]
+    return dict(w=width, h=height, mi_cols=mi_cols, mi_rows=mi_rows, sb_cols=sb_cols, sb_rows=sb_rows,
+                num_sbs=sb_cols * sb_rows, stride=stride, plane_h=plane_h, offset=offset,
+                frame_bytes=offset[2] + stride[2] * plane_h[2])
+
+
+def fwd_matrices():
+    m = np.zeros(15 * 4096, np.int32)
+    lib().mav1cu_build_fwd_matrices(m.ctypes.data)
+    return m
+
+
+class Session:
+    """Device state of one encoder instance (mav1cu_session)."""
+
+    def __init__(self, width, height, max_cdef_presets=4):
+        self.lib = lib()
+        self.geom = geometry(width, height)
+        h = ctypes.c_void_p()
+        err = ctypes.create_string_buffer(512)
+        rc = self.lib.mav1cu_session_create(width, height, max_cdef_presets, ctypes.byref(h), err, 512)
+        if rc != 0:
+            raise Mav1cuError(f"mav1cu_session_create: {err.value.decode()} ({rc})")
+        self.h = h
+
+    def close(self):
+        if self.h:
+            self.lib.mav1cu_session_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc, what):
+        if rc != 0:
+            raise Mav1cuError(f"{what}: {self.lib.mav1cu_error_string(self.h).decode()} ({rc})")
+
+    def size(self, buf):
+        return self.lib.mav1cu_buf_size(self.h, BUF[buf])
+
+    def device_ptr(self, buf):
+        return self.lib.mav1cu_buf_device(self.h, BUF[buf])
+
+    def set_stream(self, stream_ptr):
+        self.lib.mav1cu_set_stream(self.h, stream_ptr)
+
+    def upload(self, buf, arr):
+        arr = np.ascontiguousarray(arr)
+        self._check(self.lib.mav1cu_upload(self.h, BUF[buf], arr.ctypes.data, arr.nbytes), f"upload {buf}")
+
+    def download(self, buf, dtype=np.uint8, count=None, out=None):
+        if out is None:
+            n = self.size(buf) // np.dtype(dtype).itemsize if count is None else count
+            out = np.empty(n, dtype)
+        self._check(self.lib.mav1cu_download(self.h, BUF[buf], out.ctypes.data, out.nbytes), f"download {buf}")
+        self.synchronize()
+        return out
+
+    def copy(self, dst, src, nbytes=None):
+        n = min(self.size(dst), self.size(src)) if nbytes is None else nbytes
+        self._check(self.lib.mav1cu_copy(self.h, BUF[dst], BUF[src], n), "copy")
+
+    def set_params(self, params):
+        p = np.ascontiguousarray(params)
+        assert p.nbytes == 392
+        self._check(self.lib.mav1cu_set_params(self.h, p.ctypes.data), "set_params")
+
+    def motion_search(self):
+        self._check(self.lib.mav1cu_motion_search(self.h), "motion_search")
+
+    def analyze(self):
+        self._check(self.lib.mav1cu_analyze(self.h), "analyze")
+
+    def edge_types(self):
+        self._check(self.lib.mav1cu_edge_types(self.h), "edge_types")
+
+    def recon(self):
+        self._check(self.lib.mav1cu_recon(self.h), "recon")
+
+    def frame_core(self):
+        self._check(self.lib.mav1cu_frame_core(self.h), "frame_core")
+
+    def filter_info(self):
+        self._check(self.lib.mav1cu_filter_info(self.h), "filter_info")
+
+    def filter(self, num_cdef_presets):
+        self._check(self.lib.mav1cu_filter(self.h, num_cdef_presets), "filter")
+
+    def cdef_select(self, num_cdef_presets):
+        self._check(self.lib.mav1cu_cdef_select(self.h, num_cdef_presets), "cdef_select")
+
+    def restore(self):
+        self._check(self.lib.mav1cu_restore(self.h), "restore")
+
+    def synchronize(self):
+        self._check(self.lib.mav1cu_synchronize(self.h), "synchronize")
+
+    def launches(self):
+        return self.lib.mav1cu_launch_count(self.h)

@@ -1,0 +1,231 @@
+"""Stage-level parity harness: replays the oracle's per-frame backend inputs
+through the CUDA stages (via the C ABI) and compares every output with the
+oracle's, field by field. Each stage gets the oracle's own inputs, so a
+mismatch is attributed to exactly one stage."""
+import numpy as np
+
+import mav1cu
+import oracle
+import synthetic
+from mav1cu import BLOCK_DTYPE, PARAMS_DTYPE, SB_DTYPE
+
+ST = oracle.STAGE
+NUM_NODES, A_SLOTS = 85, 13
+
+
+def trace_clip(spec, nframes, **flags):
+    frames = list(synthetic.generate(spec, nframes))
+    cfg = oracle.cli_config(spec.width, spec.height, **flags)
+    tr = oracle.Trace()
+    packets, recons = oracle.encode(frames, cfg, trace=tr)
+    return tr, cfg, frames, packets, recons
+
+
+def params_of(fr):
+    return fr[(ST["PARAMS"], "PARAMS")][:392].copy()
+
+
+def level_slots(p, level):
+    turbo_square = (p["turbo"] & 1) and (not p["frame_is_intra"] or (p["turbo"] & 256))
+    if level == 3 or turbo_square:
+        return 1
+    if level == 2 or p["fast"]:
+        return 5
+    return A_SLOTS
+
+
+def node_base(level):
+    return (0, 1, 5, 21)[level]
+
+
+class FrameCheck:
+    """Runs the CUDA stages of one traced frame against the oracle's snapshots."""
+
+    def __init__(self, sess, tr, cfg, fr):
+        self.s, self.tr, self.cfg, self.fr = sess, tr, cfg, fr
+        self.g = tr.geom
+        self.fb = self.g["frame_bytes"]
+        self.nsb = self.g["num_sbs"]
+        self.params = params_of(fr)
+        self.p = self.params.view(PARAMS_DTYPE)[0]
+        self.state = fr["state"]
+
+    def snap(self, stage, name, nbytes=None):
+        a = self.fr[(ST[stage], name)]
+        return a if nbytes is None else a[:nbytes]
+
+    def frame_inputs(self):
+        s, fb = self.s, self.fb
+        s.set_params(self.params)
+        s.upload("SRC", self.snap("PARAMS", "SRC", fb))
+        s.upload("REF", self.snap("PARAMS", "REF", fb))
+        s.upload("GOLD", self.snap("PARAMS", "GOLD", fb))
+        s.upload("MATS", self.tr.mats[:15 * 4096 * 4])
+
+    # ---- per-stage checks: each returns {output: mismatch count} -------------
+    def me(self):
+        if self.p["frame_is_intra"]:
+            return {}
+        self.frame_inputs()
+        self.s.motion_search()
+        n = self.nsb * NUM_NODES * 2 * 4
+        out = {"mvfield": diff(self.s.download("MVFIELD", count=n), self.snap("ME", "MVFIELD", n))}
+        if self.p["golden"]:
+            out["mvgold"] = diff(self.s.download("MVGOLD", count=n), self.snap("ME", "MVGOLD", n))
+        return out
+
+    def analyze(self):
+        self.frame_inputs()
+        n = self.nsb * NUM_NODES * 2 * 4
+        self.s.upload("MVFIELD", self.snap("ME", "MVFIELD", n))
+        self.s.upload("MVGOLD", self.snap("ME", "MVGOLD", n))
+        self.s.analyze()
+        out = {}
+        costs = self.s.download("ACOSTS", np.int64)
+        infos = self.s.download("AINFOS", count=self.s.size("AINFOS")).view(BLOCK_DTYPE)
+        rc = self.snap("ANALYZE", "ACOSTS", self.s.size("ACOSTS")).view(np.int64)
+        ri = self.snap("ANALYZE", "AINFOS", self.s.size("AINFOS")).view(BLOCK_DTYPE)
+        idx = []
+        for level in range(4):
+            ns = level_slots(self.p, level)
+            for sb in range(self.nsb):
+                for i in range(1 << (2 * level)):
+                    base = sb * NUM_NODES * A_SLOTS + (node_base(level) + i) * A_SLOTS
+                    idx.extend(range(base, base + ns))
+        idx = np.array(idx)
+        out["acosts"] = int((costs[idx] != rc[idx]).sum())
+        live = idx[rc[idx] >= 0]
+        out["ainfos"] = blocks_diff(infos[live], ri[live], skip=("eob", "coef_off"))
+        out.update(self.blocks_sbs("ANALYZE"))
+        return out
+
+    def blocks_sbs(self, stage, sbs_ref_stage="ANALYZE"):
+        blocks = self.s.download("BLOCKS", count=self.s.size("BLOCKS")).view(BLOCK_DTYPE)
+        sbs = self.s.download("SBS", count=self.s.size("SBS")).view(SB_DTYPE)
+        rb = self.snap(stage, "BLOCKS", self.s.size("BLOCKS")).view(BLOCK_DTYPE)
+        rs = self.snap("ANALYZE", "SBS", self.s.size("SBS")).view(SB_DTYPE)
+        out = {"sbs": int((sbs != rs).sum())}
+        sel = np.concatenate([np.arange(r["first_block"], r["first_block"] + r["num_blocks"]) for r in rs])
+        out["blocks"] = blocks_diff(blocks[sel], rb[sel])
+        return out
+
+    def upload_blocks(self, stage):
+        self.s.upload("BLOCKS", self.snap(stage, "BLOCKS", self.s.size("BLOCKS")))
+        self.s.upload("SBS", self.snap("ANALYZE", "SBS", self.s.size("SBS")))
+
+    def edge(self):
+        if not self.cfg.intra_edge_filter:
+            return {}
+        self.frame_inputs()
+        self.upload_blocks("ANALYZE")
+        self.s.edge_types()
+        return {"blocks": self.blocks_sbs("EDGE")["blocks"]}
+
+    def recon(self):
+        self.frame_inputs()
+        self.upload_blocks("EDGE")
+        self.s.upload("REC", self.snap("PARAMS", "REC", self.fb))
+        self.s.upload("COEFS", self.snap("PARAMS", "COEFS", self.s.size("COEFS")))
+        self.s.recon()
+        out = {"rec": diff(self.s.download("REC", count=self.fb), self.snap("RECON", "REC", self.fb))}
+        out["coefs"] = diff(self.s.download("COEFS", np.int32), self.snap("RECON", "COEFS", self.s.size("COEFS")).view(np.int32))
+        out["blocks"] = self.blocks_sbs("RECON")["blocks"]
+        return out
+
+    def filtered(self):
+        lf_on = any(self.p["lf_level"])
+        cdef_off = (self.state["leafopt"] & 4) != 0
+        return lf_on or (self.state["num_cdef_presets"] and not cdef_off) or not self.cfg.turbo
+
+    def finfo(self):
+        if not self.filtered():
+            return {}
+        self.frame_inputs()
+        self.upload_blocks("RECON")
+        self.s.filter_info()
+        n = self.g["mi_rows"] * self.g["mi_cols"]
+        return {"lfmask": diff(self.s.download("LFMASK", count=n), self.snap("FINFO", "LFMASK", n))}
+
+    def filter(self):
+        if not self.filtered():
+            return {}
+        self.frame_inputs()
+        n = self.g["mi_rows"] * self.g["mi_cols"]
+        self.s.upload("LFMASK", self.snap("FINFO", "LFMASK", n))
+        self.s.upload("REC", self.snap("RECON", "REC", self.fb))
+        np_ = self.fr["npresets_filter"]
+        self.s.filter(np_)
+        out = {"rec": diff(self.s.download("REC", count=self.fb), self.snap("FILTER", "REC", self.fb))}
+        if np_:
+            k = np_ * self.fb
+            out["cdefbuf"] = diff(self.s.download("CDEFBUF", count=k), self.snap("FILTER", "CDEFBUF", k))
+        return out
+
+    def cdef_select(self):
+        cdef_off = (self.state["leafopt"] & 4) != 0
+        if not (self.cfg.cdef and self.cfg.qindex > 0 and not cdef_off):
+            return {}
+        self.frame_inputs()
+        self.s.upload("REC", self.snap("FILTER", "REC", self.fb))
+        np_ = self.state["num_cdef_presets"]
+        self.s.upload("CDEFBUF", self.snap("FILTER", "CDEFBUF", np_ * self.fb))
+        self.s.cdef_select(np_)
+        return {
+            "rec": diff(self.s.download("REC", count=self.fb), self.snap("CDEFSEL", "REC", self.fb)),
+            "cdef_choice": diff(self.s.download("CDEF_CHOICE", count=self.nsb), self.snap("CDEFSEL", "CDEF_CHOICE", self.nsb)),
+        }
+
+    def chain(self):
+        """Every stage on the device from the frame inputs only (the frame
+        core plus the filter chain in run_frame_core's order)."""
+        self.frame_inputs()
+        self.s.upload("REC", self.snap("PARAMS", "REC", self.fb))
+        self.s.upload("COEFS", self.snap("PARAMS", "COEFS", self.s.size("COEFS")))
+        self.s.frame_core()
+        if self.filtered():
+            self.s.filter_info()
+            self.s.filter(self.fr["npresets_filter"])
+        cdef_off = (self.state["leafopt"] & 4) != 0
+        if self.cfg.cdef and self.cfg.qindex > 0 and not cdef_off:
+            self.s.cdef_select(self.state["num_cdef_presets"])
+        out = {"rec": diff(self.s.download("REC", count=self.fb), self.snap("DONE", "REC", self.fb))}
+        out["coefs"] = diff(self.s.download("COEFS", np.int32), self.snap("RECON", "COEFS", self.s.size("COEFS")).view(np.int32))
+        out.update(self.blocks_sbs("RECON"))
+        return out
+
+
+def diff(a, b):
+    a = np.asarray(a).ravel()
+    b = np.asarray(b).ravel()[: a.size]
+    return int((a != b).sum())
+
+
+def blocks_diff(a, b, skip=()):
+    n = 0
+    for name in BLOCK_DTYPE.names:
+        if name in skip:
+            continue
+        n += int((a[name] != b[name]).sum())
+    return n
+
+
+def first_block_mismatch(a, b, skip=()):
+    for i in range(len(a)):
+        for name in BLOCK_DTYPE.names:
+            if name in skip:
+                continue
+            if np.any(a[i][name] != b[i][name]):
+                return i, name, a[i], b[i]
+    return None
+
+
+STAGES = ("me", "analyze", "edge", "recon", "finfo", "filter", "cdef_select", "chain")
+
+
+def check_all(sess, tr, cfg, stages=STAGES):
+    """[(frame index, state, {stage: {output: mismatches}})]"""
+    res = []
+    for k, fr in enumerate(tr.frames):
+        fc = FrameCheck(sess, tr, cfg, fr)
+        res.append((k, fr["state"], {st: getattr(fc, st)() for st in stages}))
+    return res
