@@ -1,0 +1,378 @@
+#!/usr/bin/env python3
+"""1080p turbo encode benchmark of the B200 encode backend.
+
+Workload (the reference's 1080p turbo configuration): a seeded synthetic
+1920x1080 8-bit 4:2:0 clip of 120 frames (pan (+2.5, +1.0) px/frame, 12
+moving rectangles of 64-256 px, noise sigma 2), coded with --turbo -q 125
+--keyint 60 --tiles 2 (deblocking and CDEF on, loop restoration off). One
+step = the whole clip in coding order (2 key frames, 58 hidden ALTREF frames,
+58 leaf frames, 2 regular frames) through every device stage of the encode
+backend: source load, motion search, mode/partition analysis, edge types,
+reconstruction, filter info, deblocking, CDEF and CDEF selection, reference
+slot refresh. Entropy coding and OBU assembly (host steps of the encoder,
+not part of this path) are not timed.
+
+value: frames/s with the source frames resident in HBM (CUDA events on the
+       session stream, max over ranks).
+e2e:   the same through the C ABI from pinned host memory: every frame's
+       source is copied host->device and its entropy-coder inputs (blocks,
+       superblock table, coefficients, CDEF choices) plus the shown frames'
+       reconstructions are copied device->host inside the timed region.
+--impl reference: the reference encoder's own scalar CPU path (oracle/_ref,
+       built from the reference sources) on the host cores, all threads.
+
+Multi-GPU: the path does not shard (one stream is a serial reference
+chain); --gpus N runs N independent replicas, one per GPU.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "mav1-encoder_b200"))
+
+import synthetic  # noqa: E402
+
+METRIC = "1080p turbo encode fps on 1 B200 (bit-exact to --cpu)"
+FLAGS = dict(q=125, turbo=1, keyint=60, tiles=2)
+SPEC = synthetic.CONFIGS["c1_1080p"]
+CONFIG = {"workload": "1920x1080 synthetic 120-frame clip, --turbo -q 125 --keyint 60 --tiles 2 (LF+CDEF on, LR off)",
+          "frames_per_step": SPEC.frames, "width": SPEC.width, "height": SPEC.height,
+          "l2": "inputs larger than L2 (373 MB of source frames per step) and a 256 MiB L2 flush between steps"}
+
+
+def load_clip(spec):
+    cache = f"/tmp/mav1cu_clip_{spec.name}_{spec.seed}_{spec.frames}.npy"
+    if os.path.exists(cache):
+        return np.load(cache)
+    frames = np.stack([np.frombuffer(synthetic.packed(f), np.uint8) for f in synthetic.generate(spec)])
+    np.save(cache, frames)
+    return frames
+
+
+class Clocks:
+    """nvidia-smi samples of SM clocks and throttle reasons during the timed region."""
+
+    def __init__(self, index):
+        self.index, self.samples, self.proc = index, [], None
+
+    def __enter__(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.samples.append([v.strip() for v in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            self.proc.wait()
+
+    def summary(self):
+        sm, mx, reasons = [], 0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for s in self.samples:
+            try:
+                sm.append(float(s[0]))
+                mx = max(mx, float(s[1]))
+                for n, v in zip(names, s[3:7]):
+                    if v.lower().startswith("active"):
+                        reasons.add(n)
+            except (ValueError, IndexError):
+                pass
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx or None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def run_ours(args, rank, world):
+    import torch
+    import mav1cu
+
+    dev = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(dev)
+    frames_host = load_clip(SPEC)
+    cfg = mav1cu.cli_config(SPEC.width, SPEC.height, **FLAGS)
+    jobs = mav1cu.plan(cfg, SPEC.frames)
+    st = mav1cu.Stream(cfg)
+    sess = st.session
+    stream = torch.cuda.Stream()
+    sess.set_stream(stream.cuda_stream)
+    frames_dev = torch.from_numpy(frames_host).to(f"cuda:{dev}")
+    fbytes = frames_host.shape[1]
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{dev}")
+    pinned = torch.from_numpy(frames_host).pin_memory()
+    geom = sess.geom
+    out_bufs = {b: torch.empty(sess.size(b), dtype=torch.uint8).pin_memory()
+                for b in ("BLOCKS", "SBS", "COEFS", "CDEF_CHOICE", "REC")}
+    d2h_per_step = 0
+
+    def step_device():
+        for j in jobs:
+            st.encode(j, frames_dev[j["disp"]].data_ptr(), True)
+
+    def step_e2e():
+        nonlocal d2h_per_step
+        d2h = 0
+        for j in jobs:
+            st.encode(j, pinned[j["disp"]].data_ptr(), False)
+            for b in ("BLOCKS", "SBS", "COEFS", "CDEF_CHOICE") + (() if j["hidden"] else ("REC",)):
+                n = sess.size(b) if b != "REC" else geom["frame_bytes"]
+                sess.lib.mav1cu_download(sess.h, mav1cu.BUF[b], out_bufs[b].data_ptr(), n)
+                d2h += n
+        d2h_per_step = d2h
+
+    def timed(fn, k, w):
+        with torch.cuda.stream(stream):
+            for _ in range(w):
+                fn()
+            stream.synchronize()
+            launches0 = sess.launches()
+            ms = []
+            for _ in range(k):
+                flush.fill_(1)
+                stream.wait_stream(torch.cuda.current_stream())
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+                fn()
+                b.record(stream)
+                b.synchronize()
+                ms.append(a.elapsed_time(b))
+            sess.synchronize()
+            return ms, (sess.launches() - launches0) // k
+
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    torch.cuda.synchronize()
+    with Clocks(dev) as clk:
+        ms, launches = timed(step_device, args.steps, args.warmup)
+    torch.cuda.synchronize()
+    ms_e2e, _ = timed(step_e2e, max(1, args.steps // 2), 1)
+    per_step = sum(ms) / len(ms)
+    per_e2e = sum(ms_e2e) / len(ms_e2e)
+    if world > 1:
+        import torch.distributed as dist
+        t = torch.tensor([per_step, per_e2e], dtype=torch.float64, device=f"cuda:{dev}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        per_step, per_e2e = t.tolist()
+    kern = kernel_times(sess, stream, step_device) if (rank == 0 and not args.no_roofline) else None
+    st.close()
+    return dict(ms=per_step, ms_e2e=per_e2e, launches=launches, clocks=clk.summary(),
+                h2d=SPEC.frames * fbytes, d2h=d2h_per_step, kern=kern)
+
+
+def kernel_times(sess, stream, step_fn):
+    """Per-kernel device time of one step, measured with CUDA events around
+    each stage of one ALTREF frame (the dominant frame kind) on the session
+    stream; used for the roofline of the dominant kernel."""
+    import torch
+    import mav1cu
+
+    # re-run one ALTREF frame stage by stage with events between stages
+    cfg = mav1cu.cli_config(SPEC.width, SPEC.height, **FLAGS)
+    jobs = mav1cu.plan(cfg, SPEC.frames)
+    arf = next(j for j in jobs if j["kind"] == 1)
+    fp, presets = mav1cu.frame_params(cfg, arf)
+    sess.set_params(fp)
+    stages = [("motion_search", sess.motion_search), ("analyze", sess.analyze), ("edge_types", sess.edge_types),
+              ("recon", sess.recon), ("filter_info", sess.filter_info), ("filter", lambda: sess.filter(presets)),
+              ("cdef_select", lambda: sess.cdef_select(4))]
+    res = {}
+    with torch.cuda.stream(stream):
+        for _ in range(3):
+            for name, fn in stages:
+                fn()
+        stream.synchronize()
+        for name, fn in stages:
+            ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+            ts = []
+            for _ in range(5):
+                ev[0].record(stream)
+                fn()
+                ev[1].record(stream)
+                ev[1].synchronize()
+                ts.append(ev[0].elapsed_time(ev[1]))
+            res[name] = statistics.median(ts)
+    return res
+
+
+def roofline(kern, peaks):
+    """Roofline of the dominant stage of an ALTREF frame: algorithmic bytes
+    (compulsory reads + writes of the stage at 1080p) over its measured time."""
+    if not kern:
+        return None
+    name = max(kern, key=kern.get)
+    fb = 3133440  # padded 1080p frame bytes
+    nsb = 510
+    alg = {  # compulsory bytes per launch of each stage (measurement section)
+        "motion_search": 3 * fb + 16 * 1920 * 1080 + nsb * 85 * 8,
+        "analyze": 3 * fb + nsb * 85 * 13 * (8 + 108) // 13 + nsb * 64 * 108,
+        "edge_types": 2 * nsb * 64 * 108,
+        "recon": 3 * fb + nsb * 64 * 108 + nsb * 6144 * 4 + 61440 * 4,
+        "filter_info": nsb * 64 * 108 + 135 * 480,
+        "filter": 2 * fb + 2 * fb + 135 * 480,
+        "cdef_select": 4 * fb + fb,
+    }[name]
+    t = kern[name] * 1e-3
+    peak = peaks.get("hbm_gbs", 6650.0)
+    achieved = alg / t / 1e9
+    return {"bound": "hbm", "kernel": name, "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+            "frac": round(achieved / peak, 5), "traffic": None, "algorithmic_bytes": alg,
+            "ms_per_launch": round(kern[name], 4), "stage_ms": {k: round(v, 4) for k, v in kern.items()},
+            "peak_source": "MEASURED_PEAKS.json" if "hbm_gbs" in peaks else "fallback"}
+
+
+def cpu_reference(args, sample_frames, per_kind=True):
+    """The reference's scalar CPU path (oracle/_ref) on the host cores: the
+    backend stages of the first `sample_frames` frames of the clip, timed per
+    frame between run_frame_core's first and last stage hook; fps of the
+    120-frame clip from the per-kind mean times weighted by the clip's kind
+    counts."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+
+    frames = [np.split(f, [SPEC.width * SPEC.height, SPEC.width * SPEC.height + ((SPEC.width + 1) // 2) * ((SPEC.height + 1) // 2)])
+              for f in load_clip(SPEC)[:sample_frames]]
+    frames = [[f[0].reshape(SPEC.height, SPEC.width), f[1].reshape((SPEC.height + 1) // 2, -1),
+               f[2].reshape((SPEC.height + 1) // 2, -1)] for f in frames]
+    cfg = oracle.cli_config(SPEC.width, SPEC.height, **FLAGS)
+    times = []
+
+    class Tr:
+        pass
+
+    tr = Tr()
+    state = {}
+
+    def hook(user, stage, e):
+        if stage == oracle.STAGE["PARAMS"]:
+            state["t0"] = time.perf_counter()
+            state["kind"] = oracle.frame_state(e)
+        elif stage == oracle.STAGE["DONE"]:
+            k = state["kind"]
+            kind = "key" if k["is_key"] else {0: "regular", 1: "arf", 2: "leaf", 3: "arf"}[k["frame_kind"]]
+            times.append((kind, time.perf_counter() - state["t0"]))
+
+    tr.cb = oracle.HOOK(hook)
+    oracle.encode(frames, cfg, trace=tr)
+    by = {}
+    for k, t in times:
+        by.setdefault(k, []).append(t)
+    mean = {k: sum(v) / len(v) for k, v in by.items()}
+    counts = {"key": 2, "arf": 58, "leaf": 58, "regular": 2}
+    total = sum(counts[k] * mean.get(k, mean.get("arf")) for k in counts)
+    return SPEC.frames / total, sum(t for _, t in times), mean
+
+
+def profile_run(n):
+    import torch
+    import mav1cu
+
+    frames_host = load_clip(SPEC)
+    cfg = mav1cu.cli_config(SPEC.width, SPEC.height, **FLAGS)
+    jobs = mav1cu.plan(cfg, SPEC.frames)[:n]
+    st = mav1cu.Stream(cfg)
+    frames_dev = torch.from_numpy(frames_host[: max(j["disp"] for j in jobs) + 1]).cuda()
+    for j in jobs:
+        st.encode(j, frames_dev[j["disp"]].data_ptr(), True)
+    st.session.synchronize()
+    print(json.dumps({"profile_frames": n, "kinds": [int(j["kind"]) for j in jobs],
+                      "launches": int(st.session.launches())}))
+    st.close()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cpu-sample", type=int, default=16, help="frames of the CPU baseline sample")
+    ap.add_argument("--no-roofline", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-frames", type=int, default=0,
+                    help="code the clip's first N planned frames once and exit (a short run for ncu)")
+    args = ap.parse_args()
+    if args.profile_frames:
+        profile_run(args.profile_frames)
+        return
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    cores = os.cpu_count()
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        per_step = []
+        for i in range(args.warmup + args.steps):
+            fps, secs, mean = cpu_reference(args, 8)
+            if i >= args.warmup:
+                per_step.append(fps)
+        v = sum(per_step) / len(per_step)
+        line = {"metric": METRIC, "value": round(v, 3), "unit": "fps", "n_gpus": args.gpus, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": round(1000 * SPEC.frames / v, 1), "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "u8/int32", "data": "synthetic",
+                "config": CONFIG, "impl": "reference",
+                "cpu_baseline": {"value": round(v, 3), "unit": "fps", "cores": cores, "kind": "reference",
+                                 "sample": "per step: the backend stages of the clip's first 8 frames (key, ALTREF and "
+                                           "leaf frames), per-kind mean time weighted to the 120-frame clip"},
+                "e2e": {"value": round(v, 3), "unit": "fps", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return
+
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+    r = run_ours(args, rank, world)
+    if rank == 0:
+        peaks = {}
+        try:
+            peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        except Exception:
+            pass
+        frames = SPEC.frames * world
+        value = frames / (r["ms"] * 1e-3)
+        e2e = frames / (r["ms_e2e"] * 1e-3)
+        line = {"metric": METRIC, "value": round(value, 2), "unit": "fps", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": round(r["ms"], 3), "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "u8/int32", "data": "synthetic", "config": CONFIG,
+                "parallelism": "replicas" if world > 1 else "single",
+                "e2e": {"value": round(e2e, 2), "unit": "fps", "h2d_bytes_per_step": r["h2d"],
+                        "d2h_bytes_per_step": r["d2h"]},
+                "gpu_launches": int(r["launches"]), "clocks": r["clocks"],
+                "roofline": roofline(r["kern"], peaks)}
+        if not args.no_cpu_baseline:
+            fps, secs, mean = cpu_reference(args, args.cpu_sample)
+            line["cpu_baseline"] = {"value": round(fps, 3), "unit": "fps", "cores": cores, "kind": "reference",
+                                    "sample": f"backend stages of the clip's first {args.cpu_sample} frames "
+                                              f"({secs:.1f} s of CPU work), per-kind mean time weighted to the 120-frame clip",
+                                    "per_kind_ms": {k: round(v * 1e3, 1) for k, v in mean.items()}}
+        print(json.dumps(line))
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -198,6 +198,84 @@ const char *mav1cu_error_string(const mav1cu_session *s);
 /* Number of kernel launches this session has enqueued since creation. */
 int64_t mav1cu_launch_count(const mav1cu_session *s);
 
+
+/* ---- encoder configuration and frame planning ---------------------------
+ * mav1cu_config has the byte layout of the reference's Mav1Config
+ * (src/mav1.h:20-42); the fields keep their meaning. */
+typedef struct {
+  int32_t width, height;
+  int32_t qindex;
+  int32_t use_metal;
+  int32_t keyint;
+  int32_t tx_search;
+  int32_t tx_depth;
+  int32_t loop_filter;
+  int32_t cdef;
+  int32_t restoration;
+  int32_t tile_cols_log2;
+  int32_t intra_edge_filter;
+  int32_t nonref_odd;
+  int32_t fast;
+  int32_t multi_ref;
+  int32_t altref;
+  int32_t leaf;
+  int32_t switchable_interp;
+  int32_t lr_test;
+  int32_t me_range;
+  int32_t threads;
+  int32_t turbo;
+} mav1cu_config;
+
+/* One coded frame of a stream, in coding order: the frame-structure
+ * decisions of the reference's driver (mav1_encode, encoder.c:822-846, and
+ * the ALTREF driver alt_drain / pyr_code / alt_code, encoder.c:1004-1293). */
+typedef struct {
+  int32_t disp;              /* display index of the source frame */
+  int32_t is_key;
+  int32_t kind;              /* 0 regular, 1 hidden ALTREF, 2 inside the mini-GOP, 3 pyramid middle */
+  int32_t last_slot;         /* reference slot of LAST (-1: none) */
+  int32_t arf_slot;          /* reference slot of the second reference (-1: none) */
+  int32_t refresh;           /* refresh_frame_flags */
+  int32_t hidden;            /* not shown (shown later by show_existing_frame) */
+  int32_t base_q_idx;
+  int32_t order_hint;
+  int32_t nonref;            /* not kept as a reference */
+  int32_t leafopt;           /* leaf-frame savings of this frame */
+  int32_t reference_select;  /* compound LAST + ALTREF allowed */
+  int32_t golden_refresh;    /* (no ALTREF) frame refreshes GOLDEN */
+  int32_t gold_differs;      /* (no ALTREF) GOLDEN holds another frame than LAST */
+  int32_t show_existing;     /* >= 0: after this frame a show_existing_frame of that slot follows */
+  int32_t pad;
+} mav1cu_frame_job;
+
+/* Normalises cfg like the reference's encoder creation (turbo implies fast,
+ * ALTREF >= 2 and leaf frames; encoder.c:69-90) and writes the coding order
+ * of a clip of nframes frames into jobs (at most cap). Returns the number of
+ * jobs, or a negative status. */
+int mav1cu_plan(const mav1cu_config *cfg, int nframes, mav1cu_frame_job *jobs, int cap);
+/* Frame parameters of one planned frame (setup_params, encoder.c:407-510).
+ * *num_cdef_presets receives the presets the filter stage writes (0 with
+ * CDEF off for the frame). */
+int mav1cu_frame_params_for(const mav1cu_config *cfg, const mav1cu_frame_job *job, mav1cu_frame_params *fp,
+                            int *num_cdef_presets);
+
+/* A device-resident stream: one session plus the reference slots (8 frame
+ * buffers in HBM); each call codes one planned frame through every device
+ * stage (source load with edge replication, frame core, filter info,
+ * deblocking, CDEF, CDEF selection, slot refresh). The frame's writer inputs
+ * (BLOCKS, SBS, COEFS, CDEF_CHOICE, PARAMS) and its reconstruction (REC) are
+ * in the session's buffers when the call's work completes. */
+typedef struct mav1cu_stream mav1cu_stream;
+int mav1cu_stream_create(const mav1cu_config *cfg, mav1cu_stream **out, char *err, size_t errlen);
+void mav1cu_stream_destroy(mav1cu_stream *st);
+mav1cu_session *mav1cu_stream_session(mav1cu_stream *st);
+/* i420: packed I420 source of the job's frame (width x height luma, then the
+ * two (w+1)/2 x (h+1)/2 chroma planes), in device memory if on_device, else
+ * in host memory (pinned for an asynchronous copy). */
+int mav1cu_stream_encode(mav1cu_stream *st, const mav1cu_frame_job *job, const void *i420, int on_device);
+/* Device address of reference slot k (0..7), frame_bytes each. */
+void *mav1cu_stream_slot(mav1cu_stream *st, int k);
+
 /* ---- host helpers (no device work) --------------------------------------- */
 /* Forward transform matrices (Q20), 15 x 4096 int32: least-squares inverses
  * of the normative inverse kernels. Replaces fwd_build_matrices

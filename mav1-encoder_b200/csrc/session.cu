@@ -20,6 +20,7 @@
 #include "analysis.cuh"
 #include "recon.cuh"
 #include "filters.cuh"
+#include "stream.cuh"
 
 namespace {
 
@@ -548,3 +549,128 @@ extern "C" int mav1cu_synchronize(mav1cu_session *s) {
 
 extern "C" const char *mav1cu_error_string(const mav1cu_session *s) { return s->err ? s->msg : ""; }
 extern "C" int64_t mav1cu_launch_count(const mav1cu_session *s) { return s->launches; }
+
+// ---- frame planning and the device-resident stream ------------------------------------
+
+extern "C" int mav1cu_plan(const mav1cu_config *cfg, int nframes, mav1cu_frame_job *jobs, int cap) {
+  if (!cfg || nframes < 0 || (nframes && !jobs)) return MAV1CU_ERR_ARG;
+  drv::Planner pl;
+  pl.n = drv::normalise(cfg);
+  if (pl.n.c.altref > 0) pl.drain(nframes);
+  else pl.low_delay(nframes);
+  int n = (int)pl.jobs.size();
+  if (n > cap) return MAV1CU_ERR_ARG;
+  for (int i = 0; i < n; i++) jobs[i] = pl.jobs[i];
+  return n;
+}
+
+extern "C" int mav1cu_frame_params_for(const mav1cu_config *cfg, const mav1cu_frame_job *job, mav1cu_frame_params *fp,
+                                       int *num_cdef_presets) {
+  if (!cfg || !job || !fp) return MAV1CU_ERR_ARG;
+  drv::Norm n = drv::normalise(cfg);
+  int presets = 0;
+  drv::frame_params(n, *job, fp, &presets);
+  if (num_cdef_presets) *num_cdef_presets = presets;
+  return MAV1CU_OK;
+}
+
+struct mav1cu_stream {
+  drv::Norm n;
+  mav1cu_session *s;
+  uint8_t *slot[8];
+  uint8_t *staging;
+  size_t i420_bytes;
+};
+
+extern "C" int mav1cu_stream_create(const mav1cu_config *cfg, mav1cu_stream **out, char *err, size_t errlen) {
+  *out = NULL;
+  drv::Norm n = drv::normalise(cfg);
+  if (n.c.restoration && n.c.qindex > 0) {
+    // run_frame_core's loop-restoration parameter search (lr_select) is a
+    // host step of the encoder; the device stream codes frames without it
+    snprintf(err, errlen, "the device stream does not run the loop-restoration search (restoration must be 0)");
+    return MAV1CU_ERR_ARG;
+  }
+  mav1cu_session *s = NULL;
+  int rc = mav1cu_session_create(n.c.width, n.c.height, 4, &s, err, errlen);
+  if (rc) return rc;
+  mav1cu_stream *st = new mav1cu_stream();
+  st->n = n;
+  st->s = s;
+  size_t fb = s->g.frame_bytes;
+  st->i420_bytes = (size_t)n.c.width * n.c.height + 2 * (size_t)((n.c.width + 1) >> 1) * ((n.c.height + 1) >> 1);
+  cudaError_t e = cudaSuccess;
+  for (int k = 0; k < 8 && e == cudaSuccess; k++) {
+    e = cudaMalloc(&st->slot[k], fb);
+    if (e == cudaSuccess) e = cudaMemset(st->slot[k], 0, fb);
+  }
+  if (e == cudaSuccess) e = cudaMalloc(&st->staging, st->i420_bytes);
+  if (e != cudaSuccess) {
+    snprintf(err, errlen, "stream allocation failed: %s", cudaGetErrorString(e));
+    mav1cu_stream_destroy(st);
+    return MAV1CU_ERR_NOMEM;
+  }
+  *out = st;
+  return MAV1CU_OK;
+}
+
+extern "C" void mav1cu_stream_destroy(mav1cu_stream *st) {
+  if (!st) return;
+  if (st->s) cudaStreamSynchronize(st->s->stream);
+  for (int k = 0; k < 8; k++)
+    if (st->slot[k]) cudaFree(st->slot[k]);
+  if (st->staging) cudaFree(st->staging);
+  mav1cu_session_destroy(st->s);
+  delete st;
+}
+
+extern "C" mav1cu_session *mav1cu_stream_session(mav1cu_stream *st) { return st->s; }
+extern "C" void *mav1cu_stream_slot(mav1cu_stream *st, int k) { return k >= 0 && k < 8 ? st->slot[k] : NULL; }
+
+// Slots the reference encoder keeps (encoder.c:129-136): ALTREF driver 0, 2, 3
+// (and 4..7 with pyramid leaf frames); low-delay path LAST 0 and GOLDEN 1.
+static int slot_exists(const drv::Norm &n, int k) {
+  if (n.c.altref) return k == 0 || k == 2 || k == 3 || (n.c.leaf && k >= 4);
+  return k == 0 || (k == 1 && n.c.multi_ref);
+}
+
+extern "C" int mav1cu_stream_encode(mav1cu_stream *st, const mav1cu_frame_job *job, const void *i420, int on_device) {
+  mav1cu_session *s = st->s;
+  if (s->err) return s->err;
+  const mav1cu_config &c = st->n.c;
+  size_t fb = s->g.frame_bytes;
+  const uint8_t *src = (const uint8_t *)i420;
+  if (!on_device) {
+    if (check_cuda(s, cudaMemcpyAsync(st->staging, i420, st->i420_bytes, cudaMemcpyHostToDevice, s->stream), "source upload"))
+      return s->err;
+    src = st->staging;
+  }
+  dim3 grid((s->g.stride[0] + 127) / 128, s->g.plane_h[0], 3);
+  drv::k_load_source<<<grid, 128, 0, s->stream>>>(src, U8(s, MAV1CU_BUF_SRC), c.width, c.height, s->g.sb_cols,
+                                                  s->g.sb_rows);
+  if (after_launch(s, "load source")) return s->err;
+  if (!job->is_key) {
+    if (job->last_slot < 0 || job->last_slot > 7) return set_error(s, MAV1CU_ERR_ARG, "stream: bad LAST slot");
+    if (check_cuda(s, cudaMemcpyAsync(s->buf[MAV1CU_BUF_REF], st->slot[job->last_slot], fb, cudaMemcpyDeviceToDevice, s->stream), "ref"))
+      return s->err;
+    if (job->arf_slot >= 0 &&
+        check_cuda(s, cudaMemcpyAsync(s->buf[MAV1CU_BUF_GOLD], st->slot[job->arf_slot], fb, cudaMemcpyDeviceToDevice, s->stream), "gold"))
+      return s->err;
+  }
+  FrameParams fp;
+  int presets = 0;
+  drv::frame_params(st->n, *job, &fp, &presets);
+  if (mav1cu_set_params(s, &fp) || mav1cu_frame_core(s)) return s->err;
+  // filter stage gating of run_frame_core (encoder.c:617-632)
+  int nPresets = c.cdef ? 4 : 0, cdefOff = (job->leafopt & 4) != 0;
+  int lfOn = fp.lf_level[0] || fp.lf_level[1] || fp.lf_level[2] || fp.lf_level[3];
+  int filt = lfOn || (nPresets && !cdefOff) || !c.turbo;
+  if (filt && (mav1cu_filter_info(s) || mav1cu_filter(s, presets))) return s->err;
+  if (c.cdef && c.qindex > 0 && !cdefOff && mav1cu_cdef_select(s, nPresets)) return s->err;
+  int rf = job->is_key ? 0xFF : job->refresh;
+  for (int k = 0; k < 8; k++)
+    if (((rf >> k) & 1) && slot_exists(st->n, k) &&
+        check_cuda(s, cudaMemcpyAsync(st->slot[k], s->buf[MAV1CU_BUF_REC], fb, cudaMemcpyDeviceToDevice, s->stream), "slot"))
+      return s->err;
+  return MAV1CU_OK;
+}

@@ -45,6 +45,13 @@ SB_DTYPE = np.dtype([("first_block", "<i4"), ("num_blocks", "<i4"), ("sb_row", "
                      ("part", "<i4", (85,))])
 LRUNIT_DTYPE = np.dtype([("type", "<i4"), ("set", "<i4"), ("xqd", "<i4", (2,)), ("wiener", "<i4", (2, 3)),
                          ("pad", "<i4", (2,))])
+CONFIG_FIELDS = ["width", "height", "qindex", "use_metal", "keyint", "tx_search", "tx_depth", "loop_filter", "cdef",
+                 "restoration", "tile_cols_log2", "intra_edge_filter", "nonref_odd", "fast", "multi_ref", "altref",
+                 "leaf", "switchable_interp", "lr_test", "me_range", "threads", "turbo"]
+CONFIG_DTYPE = np.dtype([(n, "<i4") for n in CONFIG_FIELDS])
+JOB_DTYPE = np.dtype([(n, "<i4") for n in [
+    "disp", "is_key", "kind", "last_slot", "arf_slot", "refresh", "hidden", "base_q_idx", "order_hint", "nonref",
+    "leafopt", "reference_select", "golden_refresh", "gold_differs", "show_existing", "pad"]])
 assert PARAMS_DTYPE.itemsize == 392 and BLOCK_DTYPE.itemsize == 108
 assert SB_DTYPE.itemsize == 356 and LRUNIT_DTYPE.itemsize == 48
 
@@ -53,7 +60,9 @@ EXPORTS = [
     "mav1cu_buf_device", "mav1cu_upload", "mav1cu_download", "mav1cu_copy", "mav1cu_set_params",
     "mav1cu_motion_search", "mav1cu_analyze", "mav1cu_edge_types", "mav1cu_recon", "mav1cu_frame_core",
     "mav1cu_filter_info", "mav1cu_filter", "mav1cu_cdef_select", "mav1cu_restore", "mav1cu_synchronize",
-    "mav1cu_error_string", "mav1cu_launch_count", "mav1cu_build_fwd_matrices",
+    "mav1cu_error_string", "mav1cu_launch_count", "mav1cu_build_fwd_matrices", "mav1cu_plan",
+    "mav1cu_frame_params_for", "mav1cu_stream_create", "mav1cu_stream_destroy", "mav1cu_stream_session",
+    "mav1cu_stream_encode", "mav1cu_stream_slot",
 ]
 
 
@@ -91,6 +100,20 @@ def load_library(path=LIB_PATH):
     lib.mav1cu_launch_count.restype = ctypes.c_int64
     lib.mav1cu_build_fwd_matrices.argtypes = [vp]
     lib.mav1cu_build_fwd_matrices.restype = None
+    lib.mav1cu_plan.argtypes = [vp, i32, vp, i32]
+    lib.mav1cu_plan.restype = i32
+    lib.mav1cu_frame_params_for.argtypes = [vp, vp, vp, ctypes.POINTER(i32)]
+    lib.mav1cu_frame_params_for.restype = i32
+    lib.mav1cu_stream_create.argtypes = [vp, ctypes.POINTER(vp), ctypes.c_char_p, sz]
+    lib.mav1cu_stream_create.restype = i32
+    lib.mav1cu_stream_destroy.argtypes = [vp]
+    lib.mav1cu_stream_destroy.restype = None
+    lib.mav1cu_stream_session.argtypes = [vp]
+    lib.mav1cu_stream_session.restype = vp
+    lib.mav1cu_stream_encode.argtypes = [vp, vp, vp, i32]
+    lib.mav1cu_stream_encode.restype = i32
+    lib.mav1cu_stream_slot.argtypes = [vp, i32]
+    lib.mav1cu_stream_slot.restype = vp
     return lib
 
 
@@ -216,3 +239,81 @@ class Session:
 
     def launches(self):
         return self.lib.mav1cu_launch_count(self.h)
+
+
+def cli_config(width, height, q=100, keyint=0, lf=1, cdef=1, txs=1, txd=1, lr=1, lr_test=0, sw=1, fast=0, turbo=0,
+               golden=0, altref=0, leaf=0, edge=1, tiles=-1, me_range=32):
+    """mav1cu_config as the reference CLI (tools/mav1enc.c:36-104) builds its
+    Mav1Config from the same flags (defaults of mav1_default_config)."""
+    c = np.zeros(1, CONFIG_DTYPE)[0]
+    if turbo:
+        fast = 1
+    vals = dict(width=width, height=height, qindex=q, use_metal=1, keyint=keyint, tx_search=txs, tx_depth=txd,
+                loop_filter=lf, cdef=cdef, restoration=lr, lr_test=lr_test, switchable_interp=sw, me_range=me_range,
+                fast=fast, turbo=turbo, multi_ref=golden, altref=altref, leaf=leaf, nonref_odd=0,
+                intra_edge_filter=edge, tile_cols_log2=tiles if tiles >= 0 else (2 if turbo else 3 if fast else 0))
+    for k, v in vals.items():
+        c[k] = v
+    if fast:
+        c["tx_search"] = c["tx_depth"] = c["restoration"] = c["switchable_interp"] = 0
+    return np.array([c], CONFIG_DTYPE)
+
+
+def plan(cfg, nframes):
+    """Coding order of a clip (mav1cu_plan): structured array of jobs."""
+    jobs = np.zeros(4 * nframes + 8, JOB_DTYPE)
+    n = lib().mav1cu_plan(cfg.ctypes.data, nframes, jobs.ctypes.data, len(jobs))
+    if n < 0:
+        raise Mav1cuError(f"mav1cu_plan: {n}")
+    return jobs[:n]
+
+
+def frame_params(cfg, job):
+    """(FrameParams as 392 raw bytes, CDEF presets the filter stage writes)."""
+    fp = np.zeros(392, np.uint8)
+    presets = ctypes.c_int()
+    j = np.array([job], JOB_DTYPE)
+    rc = lib().mav1cu_frame_params_for(cfg.ctypes.data, j.ctypes.data, fp.ctypes.data, ctypes.byref(presets))
+    if rc:
+        raise Mav1cuError(f"mav1cu_frame_params_for: {rc}")
+    return fp, presets.value
+
+
+class Stream:
+    """Device-resident stream (mav1cu_stream): planned frames coded through
+    every device stage with the reference slots in HBM."""
+
+    def __init__(self, cfg):
+        self.lib = lib()
+        self.cfg = cfg
+        h = ctypes.c_void_p()
+        err = ctypes.create_string_buffer(512)
+        rc = self.lib.mav1cu_stream_create(cfg.ctypes.data, ctypes.byref(h), err, 512)
+        if rc:
+            raise Mav1cuError(f"mav1cu_stream_create: {err.value.decode()} ({rc})")
+        self.h = h
+        self.session = Session.__new__(Session)
+        self.session.lib = self.lib
+        self.session.geom = geometry(int(cfg[0]["width"]), int(cfg[0]["height"]))
+        self.session.h = ctypes.c_void_p(self.lib.mav1cu_stream_session(h))
+        self.session.close = lambda: None
+
+    def encode(self, job, i420_ptr, on_device):
+        j = np.array([job], JOB_DTYPE)
+        rc = self.lib.mav1cu_stream_encode(self.h, j.ctypes.data, i420_ptr, 1 if on_device else 0)
+        if rc:
+            raise Mav1cuError(f"mav1cu_stream_encode: {self.lib.mav1cu_error_string(self.session.h).decode()}")
+
+    def slot_ptr(self, k):
+        return self.lib.mav1cu_stream_slot(self.h, k)
+
+    def close(self):
+        if self.h:
+            self.lib.mav1cu_stream_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -71,20 +71,22 @@ def _blur_periodic(img, sigma):
 
 def _pan_sample(tex, h, w, ox, oy):
     th, tw = tex.shape
-    ys = (np.arange(h, dtype=np.float64) + oy)[:, None]
-    xs = (np.arange(w, dtype=np.float64) + ox)[None, :]
+    ys = np.arange(h, dtype=np.float64) + oy
+    xs = np.arange(w, dtype=np.float64) + ox
     y0 = np.floor(ys)
     x0 = np.floor(xs)
-    fy = ys - y0
-    fx = xs - x0
+    fy = (ys - y0)[:, None]
+    fx = (xs - x0)[None, :]
     y0 = y0.astype(np.int64) % th
     x0 = x0.astype(np.int64) % tw
     y1 = (y0 + 1) % th
     x1 = (x0 + 1) % tw
-    a = tex[y0, x0]
-    b = tex[y0, x1]
-    c = tex[y1, x0]
-    d = tex[y1, x1]
+    r0 = tex.take(y0, axis=0)
+    r1 = tex.take(y1, axis=0)
+    a = r0.take(x0, axis=1)
+    b = r0.take(x1, axis=1)
+    c = r1.take(x0, axis=1)
+    d = r1.take(x1, axis=1)
     return (a * (1 - fx) + b * fx) * (1 - fy) + (c * (1 - fx) + d * fx) * fy
 
 
