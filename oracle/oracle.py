@@ -144,6 +144,8 @@ class Trace:
         STAGE["FINFO"]: ["LFMASK"],
         STAGE["FILTER"]: ["REC", "CDEFBUF"],
         STAGE["CDEFSEL"]: ["REC", "CDEF_CHOICE"],
+        STAGE["LRSEL"]: ["PARAMS", "LRUNITS", "DBK"],
+        STAGE["RESTORE"]: ["LROUT"],
         STAGE["DONE"]: ["REC"],
     }
 

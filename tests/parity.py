@@ -175,9 +175,22 @@ class FrameCheck:
             "cdef_choice": diff(self.s.download("CDEF_CHOICE", count=self.nsb), self.snap("CDEFSEL", "CDEF_CHOICE", self.nsb)),
         }
 
+    def restore(self):
+        if (ST["RESTORE"], "LROUT") not in self.fr:
+            return {}
+        self.frame_inputs()
+        self.s.set_params(self.fr[(ST["LRSEL"], "PARAMS")][:392].copy())
+        self.s.upload("REC", self.snap("CDEFSEL", "REC", self.fb))
+        self.s.upload("DBK", self.snap("LRSEL", "DBK", self.fb))
+        self.s.upload("LROUT", self.snap("CDEFSEL", "REC", self.fb))
+        self.s.upload("LRUNITS", self.snap("LRSEL", "LRUNITS", self.s.size("LRUNITS")))
+        self.s.restore()
+        return {"lrout": diff(self.s.download("LROUT", count=self.fb), self.snap("RESTORE", "LROUT", self.fb))}
+
     def chain(self):
-        """Every stage on the device from the frame inputs only (the frame
-        core plus the filter chain in run_frame_core's order)."""
+        """Every stage on the device from the frame inputs only, in
+        run_frame_core's order (encoder.c:599-657); loop-restoration
+        parameters come from the host search (lr_select) as in the encoder."""
         self.frame_inputs()
         self.s.upload("REC", self.snap("PARAMS", "REC", self.fb))
         self.s.upload("COEFS", self.snap("PARAMS", "COEFS", self.s.size("COEFS")))
@@ -185,10 +198,20 @@ class FrameCheck:
         if self.filtered():
             self.s.filter_info()
             self.s.filter(self.fr["npresets_filter"])
+        use_lr = (ST["RESTORE"], "LROUT") in self.fr
+        if use_lr:
+            self.s.copy("DBK", "REC")
         cdef_off = (self.state["leafopt"] & 4) != 0
         if self.cfg.cdef and self.cfg.qindex > 0 and not cdef_off:
             self.s.cdef_select(self.state["num_cdef_presets"])
-        out = {"rec": diff(self.s.download("REC", count=self.fb), self.snap("DONE", "REC", self.fb))}
+        final = "REC"
+        if use_lr:
+            self.s.set_params(self.fr[(ST["LRSEL"], "PARAMS")][:392].copy())
+            self.s.upload("LRUNITS", self.snap("LRSEL", "LRUNITS", self.s.size("LRUNITS")))
+            self.s.copy("LROUT", "REC")
+            self.s.restore()
+            final = "LROUT"
+        out = {"rec": diff(self.s.download(final, count=self.fb), self.snap("DONE", "REC", self.fb))}
         out["coefs"] = diff(self.s.download("COEFS", np.int32), self.snap("RECON", "COEFS", self.s.size("COEFS")).view(np.int32))
         out.update(self.blocks_sbs("RECON"))
         return out
@@ -219,7 +242,7 @@ def first_block_mismatch(a, b, skip=()):
     return None
 
 
-STAGES = ("me", "analyze", "edge", "recon", "finfo", "filter", "cdef_select", "chain")
+STAGES = ("me", "analyze", "edge", "recon", "finfo", "filter", "cdef_select", "restore", "chain")
 
 
 def check_all(sess, tr, cfg, stages=STAGES):
