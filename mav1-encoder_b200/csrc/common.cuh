@@ -153,6 +153,16 @@ HD int floor_log2(int x) {
   return s;
 }
 
+// Sample read of a frame written during the same launch by other CTAs: through
+// L2 (L1 is not coherent across SMs within a launch).
+HD int ldpx(const uint8_t *p) {
+#if defined(__CUDA_ARCH__)
+  return __ldcg(p);
+#else
+  return *p;
+#endif
+}
+
 HD int block_w(int bs) { return 4 * T(Num_4x4_Blocks_Wide)[bs]; }
 HD int block_h(int bs) { return 4 * T(Num_4x4_Blocks_High)[bs]; }
 

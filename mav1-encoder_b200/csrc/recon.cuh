@@ -11,11 +11,15 @@
 // B200 mapping. An inter block's prediction reads only reference pictures,
 // so every inter block of the frame is coded in one launch (phase 0: one
 // CTA per superblock, all superblocks at once). Intra blocks read their
-// reconstructed neighbours: they run in superblock waves (phase 1), wave
-// (c - tileStart) + 2r, which orders every superblock after its left and
-// above-right neighbours in its tile column, exactly the reference's
-// dependency; inside a superblock the blocks run in decode order and the
-// inter blocks only mark their BlockDecoded flags. Within a transform block
+// reconstructed neighbours: a superblock's intra blocks may start once its
+// left and above-right neighbours in its tile column are complete, the
+// reference's dependency (backend_cpu.c:76-86). Phase 1 is one persistent
+// launch whose CTAs claim superblocks in wave order ((c - tileStart) + 2r)
+// and wait on per-superblock completion flags, so a superblock without
+// intra blocks costs nothing and unrelated chains proceed independently;
+// inside a superblock the blocks run in decode order and the inter blocks
+// only mark their BlockDecoded flags. Samples of the frame being written
+// are read through L2 (ldpx), as other CTAs write them during the launch. Within a transform block
 // the CTA's 256 threads split the residual, both matrix passes (64-bit
 // accumulation), the quantiser, the eob search (a max over inverse-scan
 // positions), the row / column inverse kernels and the reconstruction.
@@ -54,6 +58,13 @@ struct Ctx {
   int *status;
 };
 
+#define TILE_Y_W 129  // luma tile: x in [-1, 128), y in [-1, 64) relative to the superblock
+#define TILE_Y_H 65
+#define TILE_C_W 65   // chroma tile: x in [-1, 64), y in [-1, 32)
+#define TILE_C_H 33
+#define TILE_Y_BYTES (TILE_Y_W * TILE_Y_H)
+#define TILE_C_BYTES (TILE_C_W * TILE_C_H)
+
 struct Smem {
   int32_t resid[64 * 64];  // residual, then the inverse transform's plane
   int32_t tmp[64 * 32];    // forward row pass output
@@ -68,6 +79,14 @@ struct Smem {
   BlockInfo blk;
   int maxLumaW, maxLumaH;
   int flag;
+  // views of the reconstruction: plane origins (absolute plane coordinates)
+  // and strides; the global frame in phase 0, the superblock tile below in
+  // phase 1
+  uint8_t *recp[3];
+  int rstride[3];
+  // phase 1: the superblock's samples with a one-sample top / left halo and
+  // the above row extended over the above-right superblock
+  uint8_t tile[TILE_Y_BYTES + 2 * TILE_C_BYTES];
 };
 
 #define BD(sm, p, y, x) (sm).bd[(p) * BD_DIM * BD_DIM + ((y) + 1) * BD_DIM + ((x) + 1)]
@@ -97,7 +116,10 @@ struct CtaSync {
 
 // Levels of a candidate -> reconstruction residual (spec 7.13.3 with the
 // dequantisation of 7.12.3), into sm.resid (stride 64).
-__device__ void inverse_2d(Smem &sm, const int32_t *q, int txSz, int txType, int dcQ, int acQ) {
+// With rec set, the column pass adds its output straight into the
+// reconstruction (flipped for FLIPADST types) instead of storing it.
+__device__ void inverse_2d(Smem &sm, const int32_t *q, int txSz, int txType, int dcQ, int acQ, uint8_t *rec = nullptr,
+                           int rs = 0, int x = 0, int y = 0) {
   int lw = T(Tx_Width_Log2)[txSz], lh = T(Tx_Height_Log2)[txSz];
   int w = 1 << lw, h = 1 << lh, tw = imin(32, w), th = imin(32, h);
   int rowShift = T(Transform_Row_Shift)[txSz], denom = tx::dq_denom(txSz);
@@ -120,18 +142,27 @@ __device__ void inverse_2d(Smem &sm, const int32_t *q, int txSz, int txType, int
     for (int j = 0; j < w; j++) sm.resid[i * 64 + j] = clip3(-(1 << 15), (1 << 15) - 1, round2(t[j], rowShift));
   }
   __syncthreads();
+  int fud = tx::flip_ud(txType), flr = tx::flip_lr(txType);
   for (int j = threadIdx.x; j < w; j += RT) {
     int32_t t[64];
     for (int i = 0; i < h; i++) t[i] = sm.resid[i * 64 + j];
     tx::inverse_1d(t, ck, lh, 16);
-    for (int i = 0; i < h; i++) sm.resid[i * 64 + j] = round2(t[i], 4);
+    if (rec) {
+      uint8_t *col = rec + y * rs + x + (flr ? (w - 1 - j) : j);
+      for (int i = 0; i < h; i++) {
+        uint8_t *o = col + (fud ? (h - 1 - i) : i) * rs;
+        *o = (uint8_t)clip1((int)*o + round2(t[i], 4));
+      }
+    } else {
+      for (int i = 0; i < h; i++) sm.resid[i * 64 + j] = round2(t[i], 4);
+    }
   }
   __syncthreads();
 }
 
 // Transform, quantise and reconstruct one transform block whose prediction
 // is in `rec` (code_tx_block, k_recon.h:60-173). Returns the eob.
-__device__ int code_tx(const Ctx &c, Smem &sm, const uint8_t *src, uint8_t *rec, int stride, int x, int y, int txSz,
+__device__ int code_tx(const Ctx &c, Smem &sm, const uint8_t *src, int stride, uint8_t *rec, int rs, int x, int y, int txSz,
                        int plane, const int *cands, int numCands, int32_t *coefOut, int *outType, long long *outCost) {
   const FrameParams *fp = c.fp;
   int lw = T(Tx_Width_Log2)[txSz], lh = T(Tx_Height_Log2)[txSz];
@@ -143,7 +174,7 @@ __device__ int code_tx(const Ctx &c, Smem &sm, const uint8_t *src, uint8_t *rec,
     if (tid == 0) {
       int r[16], t[16];
       for (int i = 0; i < 4; i++)
-        for (int j = 0; j < 4; j++) r[i * 4 + j] = (int)src[(y + i) * stride + x + j] - (int)rec[(y + i) * stride + x + j];
+        for (int j = 0; j < 4; j++) r[i * 4 + j] = (int)src[(y + i) * stride + x + j] - (int)rec[(y + i) * rs + x + j];
       for (int j = 0; j < 4; j++) {
         int a1 = r[0 * 4 + j], b1 = r[1 * 4 + j], c1 = r[2 * 4 + j], d1 = r[3 * 4 + j];
         a1 += b1;
@@ -188,7 +219,7 @@ __device__ int code_tx(const Ctx &c, Smem &sm, const uint8_t *src, uint8_t *rec,
         }
         for (int i = 0; i < 4; i++)
           for (int j = 0; j < 4; j++) {
-            int o = (y + i) * stride + x + j;
+            int o = (y + i) * rs + x + j;
             rec[o] = (uint8_t)clip1((int)rec[o] + rr[i][j]);
           }
       }
@@ -215,8 +246,7 @@ __device__ int code_tx(const Ctx &c, Smem &sm, const uint8_t *src, uint8_t *rec,
     for (int k = tid; k < h * w; k += RT) {
       int i = k >> lw, j = k & (w - 1);
       int yy = fud ? (h - 1 - i) : i, xx = flr ? (w - 1 - j) : j;
-      int o = (y + yy) * stride + x + xx;
-      sm.resid[i * 64 + j] = (int)src[o] - (int)rec[o];
+      sm.resid[i * 64 + j] = (int)src[(y + yy) * stride + x + xx] - (int)rec[(y + yy) * rs + x + xx];
     }
     __syncthreads();
     const int32_t *Mh = c.mats + fwd_slot(tx::row_kind(t), lw), *Mv = c.mats + fwd_slot(tx::col_kind(t), lh);
@@ -229,7 +259,7 @@ __device__ int code_tx(const Ctx &c, Smem &sm, const uint8_t *src, uint8_t *rec,
     }
     __syncthreads();
     const int16_t *inv = d_inv_scan + d_inv_scan_off[scan_class(t)][txSz];
-    int myEob = 0;
+    int myEob = 0, myNz = 0;
     for (int k = tid; k < th * tw; k += RT) {
       int k2 = k / tw, kk = k % tw;
       const int32_t *m = Mv + k2 * h;
@@ -241,17 +271,19 @@ __device__ int code_tx(const Ctx &c, Smem &sm, const uint8_t *src, uint8_t *rec,
       int first = k == 0;
       int lv = tx::quant_level(v, first ? dcQ : acQ, first ? 26 : 22, denom, first ? invDc : invAc);
       sm.q[k] = lv;
-      if (lv != 0) myEob = imax(myEob, inv[k] + 1);
+      myNz |= lv != 0;
+      if (!single && lv != 0) myEob = imax(myEob, inv[k] + 1);
+    }
+    if (single) {
+      // only "has coefficients" matters here (the writer derives the eob)
+      int nz = __syncthreads_or(myNz);
+      for (int k = tid; k < tw * th; k += RT) coefOut[k] = sm.q[k];
+      if (nz) inverse_2d(sm, sm.q, txSz, t, dcQ, acQ, rec, rs, x, y);
+      *outType = nz ? t : DCT_DCT;
+      *outCost = 0;
+      return nz;
     }
     int eob = cta_max(myEob, sm);  // includes the barrier after the quantiser
-    if (single) {
-      if (eob > 0) inverse_2d(sm, sm.q, txSz, t, dcQ, acQ);
-      bestCost = 0;
-      bestType = eob > 0 ? t : DCT_DCT;
-      bestEob = eob;
-      qsrc = sm.q;
-      continue;
-    }
     long long sse = 0;
     if (eob > 0) {
       // keep the residual-free path's SSE source intact: the inverse reuses resid
@@ -259,8 +291,7 @@ __device__ int code_tx(const Ctx &c, Smem &sm, const uint8_t *src, uint8_t *rec,
       for (int k = tid; k < h * w; k += RT) {
         int i = k >> lw, j = k & (w - 1);
         int yy = fud ? (h - 1 - i) : i, xx = flr ? (w - 1 - j) : j;
-        int o = (y + yy) * stride + x + xx;
-        int d = (int)src[o] - clip1((int)rec[o] + sm.resid[i * 64 + j]);
+        int d = (int)src[(y + yy) * stride + x + xx] - clip1((int)rec[(y + yy) * rs + x + xx] + sm.resid[i * 64 + j]);
         sse += d * d;
       }
     } else {
@@ -300,7 +331,7 @@ __device__ int code_tx(const Ctx &c, Smem &sm, const uint8_t *src, uint8_t *rec,
     for (int k = tid; k < h * w; k += RT) {
       int i = k >> lw, j = k & (w - 1);
       int yy = fud ? (h - 1 - i) : i, xx = flr ? (w - 1 - j) : j;
-      int o = (y + yy) * stride + x + xx;
+      int o = (y + yy) * rs + x + xx;
       rec[o] = (uint8_t)clip1((int)rec[o] + sm.resid[i * 64 + j]);
     }
   }
@@ -369,8 +400,9 @@ __device__ long long code_plane(const Ctx &c, Smem &sm, int plane, int txSz) {
   int planeSz = T(Subsampled_Size)[bs][sub][sub];
   int num4x4W = T(Num_4x4_Blocks_Wide)[planeSz], num4x4H = T(Num_4x4_Blocks_High)[planeSz];
   int baseX = (MiCol >> sub) * 4, baseY = (MiRow >> sub) * 4;
-  int stride = fp->stride[plane];
-  uint8_t *px = c.rec + fp->offset[plane];
+  int stride = fp->stride[plane];           // source
+  uint8_t *px = sm.recp[plane];             // reconstruction view
+  int rs = sm.rstride[plane];
   const uint8_t *spx = c.src + fp->offset[plane];
   int stepX = T(Tx_Width)[txSz] >> 2, stepY = T(Tx_Height)[txSz] >> 2;
   int cands[16], numCands = 0;
@@ -412,27 +444,28 @@ __device__ long long code_plane(const Ctx &c, Smem &sm, int plane, int txSz) {
         a.filterType = (b.interp_filter >> (plane == 0 ? 4 : 5)) & 1;
         pred::IntraState st;
         pred::intra_state(a, &st);
-        pred::intra_edges(px, stride, startX, startY, a, st, above, left, etmp, (int)threadIdx.x, RT, CtaSync());
+        pred::intra_edges(px, rs, startX, startY, a, st, above, left, etmp, (int)threadIdx.x, RT, CtaSync());
         int tw = 1 << a.log2W, th = 1 << a.log2H;
         int dcv = a.mode == DC_PRED ? pred::intra_dc(a, above, left) : 0;
-        uint8_t *d = px + startY * stride + startX;
+        uint8_t *d = px + startY * rs + startX;
         for (int k = threadIdx.x; k < tw * th; k += RT) {
           int i = k >> a.log2W, j = k & (tw - 1);
-          d[i * stride + j] = (uint8_t)(a.mode == DC_PRED ? dcv : pred::intra_pixel(a, st, above, left, i, j));
+          d[i * rs + j] = (uint8_t)(a.mode == DC_PRED ? dcv : pred::intra_pixel(a, st, above, left, i, j));
         }
         __syncthreads();
         if (isCfl) {
-          const uint8_t *luma = c.rec + fp->offset[0];
+          const uint8_t *luma = sm.recp[0];
+          int ls = sm.rstride[0];
           int alpha, avg;
           if (txIdx > 0) {
             alpha = plane == 1 ? b.cfl_alpha_u : b.cfl_alpha_v;
             int n = tw * th;
             long long sum = 0;
             for (int k = threadIdx.x; k < n; k += RT)
-              sum += pred::cfl_luma(luma, fp->stride[0], startX, startY, sm.maxLumaW, sm.maxLumaH, k >> a.log2W, k & (tw - 1));
+              sum += pred::cfl_luma(luma, ls, startX, startY, sm.maxLumaW, sm.maxLumaH, k >> a.log2W, k & (tw - 1));
             avg = round2((int)cta_sum64(sum, sm), a.log2W + a.log2H);
           } else {
-            alpha = cfl_alpha(sm, luma, fp->stride[0], startX, startY, sm.maxLumaW, sm.maxLumaH, a.log2W, a.log2H, dcv,
+            alpha = cfl_alpha(sm, luma, ls, startX, startY, sm.maxLumaW, sm.maxLumaH, a.log2W, a.log2H, dcv,
                               spx + startY * stride + startX, stride, plane == 2 && b.cfl_alpha_u == 0, &avg);
             if (threadIdx.x == 0) {
               if (plane == 1) b.cfl_alpha_u = alpha;
@@ -441,8 +474,8 @@ __device__ long long code_plane(const Ctx &c, Smem &sm, int plane, int txSz) {
           }
           for (int k = threadIdx.x; k < tw * th; k += RT) {
             int i = k >> a.log2W, j = k & (tw - 1);
-            int v = pred::cfl_luma(luma, fp->stride[0], startX, startY, sm.maxLumaW, sm.maxLumaH, i, j);
-            d[i * stride + j] = (uint8_t)pred::cfl_pixel(dcv, alpha, v, avg);
+            int v = pred::cfl_luma(luma, ls, startX, startY, sm.maxLumaW, sm.maxLumaH, i, j);
+            d[i * rs + j] = (uint8_t)pred::cfl_pixel(dcv, alpha, v, avg);
           }
           __syncthreads();
         }
@@ -453,7 +486,7 @@ __device__ long long code_plane(const Ctx &c, Smem &sm, int plane, int txSz) {
       }
       int t = DCT_DCT;
       long long cst = 0;
-      int eob = code_tx(c, sm, spx, px, stride, startX, startY, txSz, plane, cands, numCands,
+      int eob = code_tx(c, sm, spx, stride, px, rs, startX, startY, txSz, plane, cands, numCands,
                         c.coefs + b.coef_off[plane] + txIdx * T(Tx_Width)[txSz] * T(Tx_Height)[txSz], &t, &cst);
       total += cst;
       if (threadIdx.x == 0) {
@@ -496,7 +529,7 @@ __device__ void mark_bd_inter(const FrameParams *fp, Smem &sm, const BlockInfo &
 }
 
 // One block (recon_block, k_recon.h:293-394); sm.blk holds it.
-__device__ void recon_block(const Ctx &c, Smem &sm) {
+__device__ void recon_block(const Ctx &c, Smem &sm, BlockInfo *gb) {
   const FrameParams *fp = c.fp;
   BlockInfo &b = sm.blk;
   int bs = b.bsize;
@@ -513,8 +546,8 @@ __device__ void recon_block(const Ctx &c, Smem &sm) {
   int tid = threadIdx.x;
   if (b.is_inter && fp->switchable_interp && !comp) {
     int w = block_w(bs), h = block_h(bs);
-    int x0 = MiCol * 4, y0 = MiRow * 4, stride = fp->stride[0];
-    uint8_t *px = c.rec + fp->offset[0] + y0 * stride + x0;
+    int x0 = MiCol * 4, y0 = MiRow * 4, stride = fp->stride[0], rs = sm.rstride[0];
+    uint8_t *px = sm.recp[0] + y0 * rs + x0;
     const uint8_t *sp = c.src + fp->offset[0] + y0 * stride + x0;
     int vw = imin(w, fp->frame_w - x0), vh = imin(h, fp->frame_h - y0);
     long long best = -1;
@@ -528,7 +561,7 @@ __device__ void recon_block(const Ctx &c, Smem &sm) {
       for (int k = tid; k < w * h; k += RT) {
         int i = k / w, j = k % w;
         int v = pred::inter_pixel(&ip, i, j);
-        px[i * stride + j] = (uint8_t)v;
+        px[i * rs + j] = (uint8_t)v;
         if (i < vh && j < vw) {
           int d = v - (int)sp[i * stride + j];
           sse += d * d;
@@ -549,7 +582,8 @@ __device__ void recon_block(const Ctx &c, Smem &sm) {
     int baseX = (MiCol >> sub) * 4, baseY = (MiRow >> sub) * 4;
     if (b.is_inter) {
       int w = block_w(bs) >> sub, h = block_h(bs) >> sub;
-      uint8_t *d = c.rec + fp->offset[plane] + baseY * stride + baseX;
+      int rs = sm.rstride[plane];
+      uint8_t *d = sm.recp[plane] + baseY * rs + baseX;
       pred::Inter p0, p1;
       pred::inter_setup(&p0, ref + fp->offset[plane], stride, fp->frame_w, fp->frame_h, baseX, baseY, w, h, b.mv_row,
                         b.mv_col, sub, sub, b.interp_filter);
@@ -560,7 +594,7 @@ __device__ void recon_block(const Ctx &c, Smem &sm) {
         int i = k / w, j = k % w;
         int v = comp ? clip1(round2(pred::inter_raw(&p0, i, j) + pred::inter_raw(&p1, i, j), 5))
                      : pred::inter_pixel(&p0, i, j);
-        d[i * stride + j] = (uint8_t)v;
+        d[i * rs + j] = (uint8_t)v;
       }
       __syncthreads();
     }
@@ -580,8 +614,9 @@ __device__ void recon_block(const Ctx &c, Smem &sm) {
     // tx_depth RD search: every depth from the same pixels and BlockDecoded
     // flags, the winner re-coded last unless it already was
     int w = block_w(bs), h = block_h(bs);
-    uint8_t *px = c.rec + fp->offset[0] + baseY * stride + baseX;
-    for (int k = tid; k < w * h; k += RT) sm.save[k] = px[(k / w) * stride + (k % w)];
+    int rs = sm.rstride[0];
+    uint8_t *px = sm.recp[0] + baseY * rs + baseX;
+    for (int k = tid; k < w * h; k += RT) sm.save[k] = px[(k / w) * rs + (k % w)];
     for (int k = tid; k < BD_DIM * BD_DIM; k += RT) sm.bdsave[k] = sm.bd[k];
     __syncthreads();
     long long best = -1;
@@ -590,7 +625,7 @@ __device__ void recon_block(const Ctx &c, Smem &sm) {
       int depth = d <= maxDepth ? d : bestD;
       if (d == maxDepth + 1 && bestD == maxDepth) break;
       if (d > 0) {
-        for (int k = tid; k < w * h; k += RT) px[(k / w) * stride + (k % w)] = sm.save[k];
+        for (int k = tid; k < w * h; k += RT) px[(k / w) * rs + (k % w)] = sm.save[k];
         for (int k = tid; k < BD_DIM * BD_DIM; k += RT) sm.bd[k] = sm.bdsave[k];
         __syncthreads();
       }
@@ -604,6 +639,7 @@ __device__ void recon_block(const Ctx &c, Smem &sm) {
     if (tid == 0) b.tx_depth = bestD;
     __syncthreads();
   }
+  if (tid == 0) *gb = b;
 }
 
 // clear_block_decoded_flags( r, c, 16 ) (k_recon.h:402-414).
@@ -627,14 +663,58 @@ __device__ void clear_bd(const FrameParams *fp, Smem &sm, int r, int c) {
   __syncthreads();
 }
 
-// phase 0: every inter block of superblock sbList[blockIdx.x] (or blockIdx.x);
-// phase 1: its intra blocks in decode order with BlockDecoded tracking.
-__global__ void __launch_bounds__(RT) k_recon(Ctx c, const int *sbList, int phase) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  Smem &sm = *(Smem *)smem_raw;
+// Stages the superblock's reconstruction (final inter samples, the
+// neighbours' samples) into the shared tile and points the views at it; the
+// tile covers every sample intra prediction of the superblock can read (the
+// row above, extended over the above-right superblock, and the column to the
+// left). Loads go through L2: other CTAs of the launch wrote those samples.
+__device__ void tile_load(const Ctx &c, Smem &sm, int sbRow, int sbCol) {
   const FrameParams *fp = c.fp;
-  int sb = sbList ? sbList[blockIdx.x] : blockIdx.x;
+  for (int p = 0; p < 3; p++) {
+    int sub = p > 0, tw = sub ? TILE_C_W : TILE_Y_W, th = sub ? TILE_C_H : TILE_Y_H;
+    uint8_t *t = sm.tile + (p == 0 ? 0 : TILE_Y_BYTES + (p - 1) * TILE_C_BYTES);
+    int x0 = ((sbCol * 64) >> sub) - 1, y0 = ((sbRow * 64) >> sub) - 1;
+    int stride = fp->stride[p], ph = fp->plane_h[p];
+    const uint8_t *g = c.rec + fp->offset[p];
+    for (int k = threadIdx.x; k < tw * th; k += RT) {
+      int y = y0 + k / tw, x = x0 + k % tw;
+      t[k] = (x >= 0 && y >= 0 && x < stride && y < ph) ? (uint8_t)ldpx(g + (size_t)y * stride + x) : 0;
+    }
+    if (threadIdx.x == 0) {
+      // plane origin in tile coordinates: sample (x, y) at t[(y - y0) * tw + (x - x0)]
+      sm.recp[p] = t - ((ptrdiff_t)y0 * tw + x0);
+      sm.rstride[p] = tw;
+    }
+  }
+  __syncthreads();
+}
+
+// Writes the superblock's own samples from the tile back to the frame.
+__device__ void tile_store(const Ctx &c, Smem &sm, int sbRow, int sbCol) {
+  const FrameParams *fp = c.fp;
+  for (int p = 0; p < 3; p++) {
+    int sub = p > 0, n = 64 >> sub, tw = sub ? TILE_C_W : TILE_Y_W;
+    const uint8_t *t = sm.tile + (p == 0 ? 0 : TILE_Y_BYTES + (p - 1) * TILE_C_BYTES);
+    int x0 = (sbCol * 64) >> sub, y0 = (sbRow * 64) >> sub, stride = fp->stride[p];
+    uint8_t *g = c.rec + fp->offset[p];
+    for (int k = threadIdx.x; k < n * n; k += RT) {
+      int y = k / n, x = k % n;
+      g[(size_t)(y0 + y) * stride + x0 + x] = t[(y + 1) * tw + x + 1];
+    }
+  }
+  __syncthreads();
+}
+
+// Superblock sb, phase 0: its inter blocks; phase 1: its intra blocks in
+// decode order with BlockDecoded tracking (inter blocks only mark theirs).
+__device__ void recon_superblock(const Ctx &c, Smem &sm, int sb, int phase) {
+  const FrameParams *fp = c.fp;
   SbInfo sbi = c.sbs[sb];
+  if (phase == 0 && threadIdx.x < 3) {
+    int p = threadIdx.x;
+    sm.recp[p] = c.rec + fp->offset[p];
+    sm.rstride[p] = fp->stride[p];
+  }
   if (phase == 1) {
     if (threadIdx.x == 0) {
       int any = 0;
@@ -642,8 +722,11 @@ __global__ void __launch_bounds__(RT) k_recon(Ctx c, const int *sbList, int phas
       sm.flag = any;
     }
     __syncthreads();
-    if (!sm.flag) return;
+    int any = sm.flag;
+    __syncthreads();
+    if (!any) return;
     clear_bd(fp, sm, sbi.sb_row * 16, sbi.sb_col * 16);
+    tile_load(c, sm, sbi.sb_row, sbi.sb_col);
   }
   for (int k = 0; k < sbi.num_blocks; k++) {
     BlockInfo *gb = &c.blocks[sbi.first_block + k];
@@ -651,12 +734,86 @@ __global__ void __launch_bounds__(RT) k_recon(Ctx c, const int *sbList, int phas
     __syncthreads();
     int inter = sm.blk.is_inter;
     if (phase == 0 ? inter : !inter) {
-      recon_block(c, sm);
-      if (threadIdx.x == 0) *gb = sm.blk;
+      recon_block(c, sm, gb);
     } else if (phase == 1) {
       mark_bd_inter(fp, sm, sm.blk);
     }
     __syncthreads();
+  }
+  if (phase == 1) tile_store(c, sm, sbi.sb_row, sbi.sb_col);
+}
+
+// Phase 0 over every superblock (one CTA each): the frame's inter blocks.
+__global__ void __launch_bounds__(RT) k_recon_inter(Ctx c) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Smem &sm = *(Smem *)smem_raw;
+  recon_superblock(c, sm, blockIdx.x, 0);
+}
+
+// Dependency state of the intra phase: a claim counter over the superblock
+// order (waves, see the file comment), one completion flag per superblock,
+// and the status word (0 ok; 1 a dependency wait gave up) with an abort flag.
+struct IntraSync {
+  const int *order;  // superblocks in wave order
+  int n;
+  int *next;         // claim counter
+  int *done;         // per superblock: 1 once its intra blocks are written
+  int *status;       // [0] error code, [1] abort
+};
+
+#define SPIN_LIMIT (1 << 22)  // x ~256 ns sleeps: about a second, far above any frame's recon
+
+// Phase 1 as one persistent launch: each CTA claims the next superblock in
+// wave order, waits until its left and above-right neighbours (same tile
+// column) have completed, codes its intra blocks and publishes completion.
+// Claims are in a topological order and a claimed superblock is always held
+// by a running CTA, so every wait ends; a wait that still exceeds the limit
+// sets the status and aborts the launch instead of hanging.
+__global__ void __launch_bounds__(RT) k_recon_intra(Ctx c, IntraSync q) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Smem &sm = *(Smem *)smem_raw;
+  const FrameParams *fp = c.fp;
+  volatile int *vdone = q.done;
+  volatile int *vstatus = q.status;
+  for (;;) {
+    if (threadIdx.x == 0) {
+      int item = vstatus[1] ? q.n : atomicAdd(q.next, 1);
+      int ok = item < q.n;
+      if (ok) {
+        int sb = q.order[item];
+        int r = sb / fp->sb_cols, col = sb % fp->sb_cols;
+        int ts = (col / fp->tile_w_sb) * fp->tile_w_sb, te = imin(fp->sb_cols, ts + fp->tile_w_sb);
+        int deps[2], nd = 0;
+        if (col > ts) deps[nd++] = sb - 1;
+        if (r > 0) deps[nd++] = (r - 1) * fp->sb_cols + (col + 1 < te ? col + 1 : col);
+        for (int d = 0; d < nd && ok; d++) {
+          int spins = 0;
+          while (!vdone[deps[d]]) {
+            if (vstatus[1] || ++spins > SPIN_LIMIT) {
+              if (!vstatus[1]) {
+                atomicExch(q.status, 1);
+                atomicExch(q.status + 1, 1);
+              }
+              ok = 0;
+              break;
+            }
+            __nanosleep(256);
+          }
+        }
+        __threadfence();
+        sm.flag = ok ? sb : -1;
+      } else {
+        sm.flag = -1;
+      }
+    }
+    __syncthreads();
+    int sb = sm.flag;
+    __syncthreads();
+    if (sb < 0) return;
+    recon_superblock(c, sm, sb, 1);
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) atomicExch(q.done + sb, 1);
   }
 }
 

@@ -64,7 +64,9 @@ struct mav1cu_session {
   uint8_t *dsrc, *dref[2]; // decimated planes
   uint8_t *ys, *uvs;       // edge-type marks per mi
   int *waves;              // superblock lists of the intra waves
-  int *status;             // device status word
+  int *status;             // device status: [0] error, [1] abort, [2] claim counter
+  int *sb_done;            // per-superblock completion flags of the intra phase
+  int resident_recon;      // CTAs of the intra phase (co-resident)
   std::vector<int> wave_start, wave_len;
   int wave_tile_w;
   FrameParams fp;          // host copy of the current parameters
@@ -222,7 +224,7 @@ extern "C" void mav1cu_build_fwd_matrices(int32_t *mats) {
 static void free_all(mav1cu_session *s) {
   for (int i = 0; i < MAV1CU_BUF_COUNT; i++)
     if (s->buf[i]) cudaFree(s->buf[i]);
-  void *extra[] = {s->qp[0], s->qp[1], s->dsrc, s->dref[0], s->dref[1], s->ys, s->uvs, s->waves, s->status};
+  void *extra[] = {s->qp[0], s->qp[1], s->dsrc, s->dref[0], s->dref[1], s->ys, s->uvs, s->waves, s->status, s->sb_done};
   for (void *p : extra)
     if (p) cudaFree(p);
   if (s->own_stream) cudaStreamDestroy(s->own_stream);
@@ -269,6 +271,7 @@ extern "C" int mav1cu_session_create(int width, int height, int max_cdef_presets
   if (e == cudaSuccess) e = cudaMalloc(&s->uvs, (size_t)g.mi_rows * g.mi_cols);
   if (e == cudaSuccess) e = cudaMalloc(&s->waves, sizeof(int) * nsb);
   if (e == cudaSuccess) e = cudaMalloc(&s->status, sizeof(int) * 4);
+  if (e == cudaSuccess) e = cudaMalloc(&s->sb_done, sizeof(int) * nsb);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->own_stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) {
     snprintf(err, errlen, "device allocation failed: %s", cudaGetErrorString(e));
@@ -287,7 +290,15 @@ extern "C" int mav1cu_session_create(int width, int height, int max_cdef_presets
     mav1cu_session_destroy(s);
     return code;
   }
-  cudaFuncSetAttribute(rec::k_recon, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(rec::Smem));
+  cudaFuncSetAttribute(rec::k_recon_inter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(rec::Smem));
+  cudaFuncSetAttribute(rec::k_recon_intra, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(rec::Smem));
+  {
+    int dev = 0, sms = 0, per = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, rec::k_recon_intra, RT, sizeof(rec::Smem));
+    s->resident_recon = imax(1, sms * imax(1, per));
+  }
   cudaFuncSetAttribute(ana::k_analyze_level, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)(4 * sizeof(ana::WarpMem)));
   *out = s;
@@ -471,17 +482,23 @@ extern "C" int mav1cu_recon(mav1cu_session *s) {
   c.status = s->status;
   size_t smem = sizeof(rec::Smem);
   if (!s->fp.frame_is_intra) {
-    rec::k_recon<<<s->g.num_sbs, RT, smem, s->stream>>>(c, NULL, 0);
+    rec::k_recon_inter<<<s->g.num_sbs, RT, smem, s->stream>>>(c);
     if (after_launch(s, "recon inter blocks")) return s->err;
   }
   // leaf frames code inter blocks only (the analysis never keeps intra there)
   if (s->fp.leaf && !s->fp.frame_is_intra) return MAV1CU_OK;
-  for (size_t w = 0; w < s->wave_len.size(); w++) {
-    if (!s->wave_len[w]) continue;
-    rec::k_recon<<<s->wave_len[w], RT, smem, s->stream>>>(c, s->waves + s->wave_start[w], 1);
-    if (after_launch(s, "recon intra wave")) return s->err;
-  }
-  return MAV1CU_OK;
+  rec::IntraSync q;
+  q.order = s->waves;
+  q.n = s->g.num_sbs;
+  q.next = s->status + 2;
+  q.done = s->sb_done;
+  q.status = s->status;
+  if (check_cuda(s, cudaMemsetAsync(s->sb_done, 0, sizeof(int) * s->g.num_sbs, s->stream), "recon flags") ||
+      check_cuda(s, cudaMemsetAsync(s->status + 2, 0, sizeof(int), s->stream), "recon counter"))
+    return s->err;
+  int grid = imin(s->g.num_sbs, s->resident_recon);
+  rec::k_recon_intra<<<grid, RT, smem, s->stream>>>(c, q);
+  return after_launch(s, "recon intra blocks");
 }
 
 extern "C" int mav1cu_frame_core(mav1cu_session *s) {
@@ -544,7 +561,11 @@ extern "C" int mav1cu_restore(mav1cu_session *s) {
 
 extern "C" int mav1cu_synchronize(mav1cu_session *s) {
   if (s->err) return s->err;
-  return check_cuda(s, cudaStreamSynchronize(s->stream), "synchronize");
+  if (check_cuda(s, cudaStreamSynchronize(s->stream), "synchronize")) return s->err;
+  int st[2] = {0, 0};
+  if (check_cuda(s, cudaMemcpy(st, s->status, sizeof st, cudaMemcpyDeviceToHost), "status")) return s->err;
+  if (st[0]) return set_error(s, MAV1CU_ERR_DEVICE, "device status %d: an intra-phase dependency wait gave up", st[0]);
+  return MAV1CU_OK;
 }
 
 extern "C" const char *mav1cu_error_string(const mav1cu_session *s) { return s->err ? s->msg : ""; }
