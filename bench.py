@@ -102,6 +102,17 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def split_gops(jobs):
+    """Coding-order jobs grouped by key frame: each group is independent of
+    the others (a key frame refreshes every reference slot)."""
+    gops = []
+    for j in jobs:
+        if j["is_key"] or not gops:
+            gops.append([])
+        gops[-1].append(j)
+    return gops
+
+
 def run_ours(args, rank, world):
     import torch
     import mav1cu
@@ -111,72 +122,91 @@ def run_ours(args, rank, world):
     frames_host = load_clip(SPEC)
     cfg = mav1cu.cli_config(SPEC.width, SPEC.height, **FLAGS)
     jobs = mav1cu.plan(cfg, SPEC.frames)
-    st = mav1cu.Stream(cfg)
-    sess = st.session
-    stream = torch.cuda.Stream()
-    sess.set_stream(stream.cuda_stream)
+    gops = split_gops(jobs)
+    streams = [mav1cu.Stream(cfg) for _ in gops]
+    # round-robin over the GOPs, so every stream always has work queued
+    order = [(g, gop[i]) for i in range(max(len(x) for x in gops)) for g, gop in enumerate(gops) if i < len(gop)]
+    seq_order = [(0, j) for j in jobs]
+    S = torch.cuda.Stream()
     frames_dev = torch.from_numpy(frames_host).to(f"cuda:{dev}")
     fbytes = frames_host.shape[1]
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{dev}")
     pinned = torch.from_numpy(frames_host).pin_memory()
-    geom = sess.geom
-    out_bufs = {b: torch.empty(sess.size(b), dtype=torch.uint8).pin_memory()
-                for b in ("BLOCKS", "SBS", "COEFS", "CDEF_CHOICE", "REC")}
+    geom = mav1cu.geometry(SPEC.width, SPEC.height)
+    sizes = {b: streams[0].session.size(b) for b in ("BLOCKS", "SBS", "COEFS", "CDEF_CHOICE")}
+    sizes["REC"] = geom["frame_bytes"]
+    out_bufs = {b: torch.empty(n, dtype=torch.uint8).pin_memory() for b, n in sizes.items()}
     d2h_per_step = 0
 
-    def step_device():
-        for j in jobs:
-            st.encode(j, frames_dev[j["disp"]].data_ptr(), True)
+    def step_device(order=order):
+        for g, j in order:
+            streams[g].encode(j, frames_dev[j["disp"]].data_ptr(), True)
+
+    def step_sequential():
+        step_device(seq_order)
 
     def step_e2e():
         nonlocal d2h_per_step
         d2h = 0
-        for j in jobs:
-            st.encode(j, pinned[j["disp"]].data_ptr(), False)
+        for g, j in order:
+            sess = streams[g].encode(j, pinned[j["disp"]].data_ptr(), False)
             for b in ("BLOCKS", "SBS", "COEFS", "CDEF_CHOICE") + (() if j["hidden"] else ("REC",)):
-                n = sess.size(b) if b != "REC" else geom["frame_bytes"]
-                sess.lib.mav1cu_download(sess.h, mav1cu.BUF[b], out_bufs[b].data_ptr(), n)
-                d2h += n
+                sess.lib.mav1cu_download(sess.h, mav1cu.BUF[b], out_bufs[b].data_ptr(), sizes[b])
+                d2h += sizes[b]
         d2h_per_step = d2h
 
+    def launches():
+        return sum(st.launches() for st in streams)
+
     def timed(fn, k, w):
-        with torch.cuda.stream(stream):
-            for _ in range(w):
+        for _ in range(w):
+            with torch.cuda.stream(S):
+                for st in streams:
+                    st.wait(S.cuda_stream)
                 fn()
-            stream.synchronize()
-            launches0 = sess.launches()
-            ms = []
-            for _ in range(k):
+                for st in streams:
+                    st.join(S.cuda_stream)
+        S.synchronize()
+        l0 = launches()
+        ms = []
+        for _ in range(k):
+            with torch.cuda.stream(S):
                 flush.fill_(1)
-                stream.wait_stream(torch.cuda.current_stream())
                 a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                a.record(stream)
+                a.record(S)
+                for st in streams:
+                    st.wait(S.cuda_stream)
                 fn()
-                b.record(stream)
-                b.synchronize()
-                ms.append(a.elapsed_time(b))
-            sess.synchronize()
-            return ms, (sess.launches() - launches0) // k
+                for st in streams:
+                    st.join(S.cuda_stream)
+                b.record(S)
+            b.synchronize()
+            ms.append(a.elapsed_time(b))
+        for st in streams:
+            st.synchronize()
+        return ms, (launches() - l0) // k
 
     if world > 1:
         import torch.distributed as dist
         dist.barrier()
     torch.cuda.synchronize()
     with Clocks(dev) as clk:
-        ms, launches = timed(step_device, args.steps, args.warmup)
-    torch.cuda.synchronize()
+        ms, nlaunch = timed(step_device, args.steps, args.warmup)
+    ms_seq, _ = timed(step_sequential, max(1, args.steps // 2), 1)
     ms_e2e, _ = timed(step_e2e, max(1, args.steps // 2), 1)
     per_step = sum(ms) / len(ms)
     per_e2e = sum(ms_e2e) / len(ms_e2e)
+    per_seq = sum(ms_seq) / len(ms_seq)
     if world > 1:
         import torch.distributed as dist
-        t = torch.tensor([per_step, per_e2e], dtype=torch.float64, device=f"cuda:{dev}")
+        t = torch.tensor([per_step, per_e2e, per_seq], dtype=torch.float64, device=f"cuda:{dev}")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        per_step, per_e2e = t.tolist()
-    kern = kernel_times(sess, stream, step_device) if (rank == 0 and not args.no_roofline) else None
-    st.close()
-    return dict(ms=per_step, ms_e2e=per_e2e, launches=launches, clocks=clk.summary(),
-                h2d=SPEC.frames * fbytes, d2h=d2h_per_step, kern=kern)
+        per_step, per_e2e, per_seq = t.tolist()
+    kern = kernel_times(streams[0].session, S, None) if (rank == 0 and not args.no_roofline) else None
+    for st in streams:
+        st.close()
+    return dict(ms=per_step, ms_e2e=per_e2e, ms_seq=per_seq, launches=nlaunch, clocks=clk.summary(),
+                h2d=SPEC.frames * fbytes, d2h=d2h_per_step, kern=kern, gops=len(gops))
 
 
 def kernel_times(sess, stream, step_fn):
@@ -187,6 +217,7 @@ def kernel_times(sess, stream, step_fn):
     import mav1cu
 
     # re-run one ALTREF frame stage by stage with events between stages
+    sess.set_stream(stream.cuda_stream)
     cfg = mav1cu.cli_config(SPEC.width, SPEC.height, **FLAGS)
     jobs = mav1cu.plan(cfg, SPEC.frames)
     arf = next(j for j in jobs if j["kind"] == 1)
@@ -293,9 +324,8 @@ def profile_run(n):
     frames_dev = torch.from_numpy(frames_host[: max(j["disp"] for j in jobs) + 1]).cuda()
     for j in jobs:
         st.encode(j, frames_dev[j["disp"]].data_ptr(), True)
-    st.session.synchronize()
-    print(json.dumps({"profile_frames": n, "kinds": [int(j["kind"]) for j in jobs],
-                      "launches": int(st.session.launches())}))
+    st.synchronize()
+    print(json.dumps({"profile_frames": n, "kinds": [int(j["kind"]) for j in jobs], "launches": int(st.launches())}))
     st.close()
 
 
@@ -359,6 +389,8 @@ def main():
                 "parallelism": "replicas" if world > 1 else "single",
                 "e2e": {"value": round(e2e, 2), "unit": "fps", "h2d_bytes_per_step": r["h2d"],
                         "d2h_bytes_per_step": r["d2h"]},
+                "schedule": {"gop_parallel_streams": r["gops"], "frame_engines_per_stream": 2,
+                             "fps_one_stream": round(frames / (r["ms_seq"] * 1e-3), 2)},
                 "gpu_launches": int(r["launches"]), "clocks": r["clocks"],
                 "roofline": roofline(r["kern"], peaks)}
         if not args.no_cpu_baseline:

@@ -275,6 +275,22 @@ mav1cu_session *mav1cu_stream_session(mav1cu_stream *st);
 int mav1cu_stream_encode(mav1cu_stream *st, const mav1cu_frame_job *job, const void *i420, int on_device);
 /* Device address of reference slot k (0..7), frame_bytes each. */
 void *mav1cu_stream_slot(mav1cu_stream *st, int k);
+/* Frame engines: the stream codes reference-chain frames (key, ALTREF,
+ * regular: they refresh a slot) on engine 0 and non-reference frames on
+ * engine 1, concurrently where the slot dependencies allow. Each engine is a
+ * session with its own CUDA stream; a frame's outputs stay in its engine's
+ * session buffers until that engine codes its next frame, and work the
+ * caller enqueues on that session (mav1cu_download) is ordered after it.
+ * mav1cu_stream_session returns the engine of the last encoded frame. */
+int mav1cu_stream_engines(const mav1cu_stream *st);
+mav1cu_session *mav1cu_stream_engine(mav1cu_stream *st, int k);
+/* Every engine waits for the work enqueued on `stream` so far (wait), or
+ * `stream` waits for every engine's work so far (join): brackets for timing
+ * or ordering against other device work. */
+int mav1cu_stream_wait(mav1cu_stream *st, void *stream);
+int mav1cu_stream_join(mav1cu_stream *st, void *stream);
+/* Waits for every engine; returns the first sticky error. */
+int mav1cu_stream_synchronize(mav1cu_stream *st);
 
 /* ---- host helpers (no device work) --------------------------------------- */
 /* Forward transform matrices (Q20), 15 x 4096 int32: least-squares inverses

@@ -759,7 +759,32 @@ struct IntraSync {
   int *next;         // claim counter
   int *done;         // per superblock: 1 once its intra blocks are written
   int *status;       // [0] error code, [1] abort
+  const int *edges;  // per superblock: which of its edges an intra block touches
 };
+
+// Edge bits of a superblock's intra blocks: EDGE_L / EDGE_T mark intra blocks
+// that may read across its left / top boundary (they touch it); EDGE_R /
+// EDGE_B mark intra blocks whose samples lie along its right / bottom edge.
+enum { EDGE_L = 1, EDGE_T = 2, EDGE_R = 4, EDGE_B = 8 };
+
+// One warp per superblock.
+__global__ void k_intra_edges(const FrameParams *fp, const BlockInfo *blocks, const SbInfo *sbs, int *edges) {
+  int sb = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+  if (sb >= fp->sb_cols * fp->sb_rows) return;
+  SbInfo sbi = sbs[sb];
+  int r0 = sbi.sb_row * 16, c0 = sbi.sb_col * 16, m = 0;
+  for (int k = lane; k < sbi.num_blocks; k += 32) {
+    const BlockInfo &b = blocks[sbi.first_block + k];
+    if (b.is_inter) continue;
+    int w4 = T(Num_4x4_Blocks_Wide)[b.bsize], h4 = T(Num_4x4_Blocks_High)[b.bsize];
+    if (b.mi_col == c0) m |= EDGE_L;
+    if (b.mi_row == r0) m |= EDGE_T;
+    if (b.mi_col + w4 >= c0 + 16) m |= EDGE_R;
+    if (b.mi_row + h4 >= r0 + 16) m |= EDGE_B;
+  }
+  for (int off = 16; off > 0; off >>= 1) m |= __shfl_xor_sync(0xffffffffu, m, off);
+  if (lane == 0) edges[sb] = m;
+}
 
 #define SPIN_LIMIT (1 << 22)  // x ~256 ns sleeps: about a second, far above any frame's recon
 
@@ -783,9 +808,19 @@ __global__ void __launch_bounds__(RT) k_recon_intra(Ctx c, IntraSync q) {
         int sb = q.order[item];
         int r = sb / fp->sb_cols, col = sb % fp->sb_cols;
         int ts = (col / fp->tile_w_sb) * fp->tile_w_sb, te = imin(fp->sb_cols, ts + fp->tile_w_sb);
-        int deps[2], nd = 0;
-        if (col > ts) deps[nd++] = sb - 1;
-        if (r > 0) deps[nd++] = (r - 1) * fp->sb_cols + (col + 1 < te ? col + 1 : col);
+        // the neighbours in the tile column whose intra samples this
+        // superblock's intra blocks can read: left (left column), above-left
+        // (corner sample), above and above-right (row above); a neighbour
+        // whose touching edge holds only inter samples (final since phase 0)
+        // imposes no wait. All four precede this superblock in wave order.
+        int me = q.edges[sb], deps[4], nd = 0;
+        if (col > ts && (me & EDGE_L) && (q.edges[sb - 1] & EDGE_R)) deps[nd++] = sb - 1;
+        if (r > 0 && (me & EDGE_T)) {
+          int up = sb - fp->sb_cols;
+          if (col > ts && (q.edges[up - 1] & EDGE_B)) deps[nd++] = up - 1;
+          if (q.edges[up] & EDGE_B) deps[nd++] = up;
+          if (col + 1 < te && (q.edges[up + 1] & EDGE_B)) deps[nd++] = up + 1;
+        }
         for (int d = 0; d < nd && ok; d++) {
           int spins = 0;
           while (!vdone[deps[d]]) {

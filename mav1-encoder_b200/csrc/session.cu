@@ -10,6 +10,7 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <memory>
 #include <vector>
 
 #include "common.cuh"
@@ -66,6 +67,7 @@ struct mav1cu_session {
   int *waves;              // superblock lists of the intra waves
   int *status;             // device status: [0] error, [1] abort, [2] claim counter
   int *sb_done;            // per-superblock completion flags of the intra phase
+  int *sb_edges;           // per-superblock edge bits of its intra blocks
   int resident_recon;      // CTAs of the intra phase (co-resident)
   std::vector<int> wave_start, wave_len;
   int wave_tile_w;
@@ -224,7 +226,7 @@ extern "C" void mav1cu_build_fwd_matrices(int32_t *mats) {
 static void free_all(mav1cu_session *s) {
   for (int i = 0; i < MAV1CU_BUF_COUNT; i++)
     if (s->buf[i]) cudaFree(s->buf[i]);
-  void *extra[] = {s->qp[0], s->qp[1], s->dsrc, s->dref[0], s->dref[1], s->ys, s->uvs, s->waves, s->status, s->sb_done};
+  void *extra[] = {s->qp[0], s->qp[1], s->dsrc, s->dref[0], s->dref[1], s->ys, s->uvs, s->waves, s->status, s->sb_done, s->sb_edges};
   for (void *p : extra)
     if (p) cudaFree(p);
   if (s->own_stream) cudaStreamDestroy(s->own_stream);
@@ -272,6 +274,7 @@ extern "C" int mav1cu_session_create(int width, int height, int max_cdef_presets
   if (e == cudaSuccess) e = cudaMalloc(&s->waves, sizeof(int) * nsb);
   if (e == cudaSuccess) e = cudaMalloc(&s->status, sizeof(int) * 4);
   if (e == cudaSuccess) e = cudaMalloc(&s->sb_done, sizeof(int) * nsb);
+  if (e == cudaSuccess) e = cudaMalloc(&s->sb_edges, sizeof(int) * nsb);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->own_stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) {
     snprintf(err, errlen, "device allocation failed: %s", cudaGetErrorString(e));
@@ -493,6 +496,9 @@ extern "C" int mav1cu_recon(mav1cu_session *s) {
   q.next = s->status + 2;
   q.done = s->sb_done;
   q.status = s->status;
+  q.edges = s->sb_edges;
+  rec::k_intra_edges<<<(s->g.num_sbs + 3) / 4, 128, 0, s->stream>>>(DP(s), c.blocks, c.sbs, s->sb_edges);
+  if (after_launch(s, "intra edges")) return s->err;
   if (check_cuda(s, cudaMemsetAsync(s->sb_done, 0, sizeof(int) * s->g.num_sbs, s->stream), "recon flags") ||
       check_cuda(s, cudaMemsetAsync(s->status + 2, 0, sizeof(int), s->stream), "recon counter"))
     return s->err;
@@ -595,12 +601,30 @@ extern "C" int mav1cu_frame_params_for(const mav1cu_config *cfg, const mav1cu_fr
   return MAV1CU_OK;
 }
 
+// Frame engines: reference-chain frames (they refresh a slot) run on engine
+// 0, non-reference frames on engine 1, each with its own session and CUDA
+// stream (the reference's frame engines, encoder.c:1036-1176, with the same
+// chain / leaf split). Slot reads and writes are ordered by CUDA events: a
+// frame's reference copies wait for the slot's last write, and a slot write
+// waits for every earlier frame that copied the slot's previous picture.
+#define NUM_ENGINES 2
+
+struct Event {
+  cudaEvent_t e;
+  Event() { cudaEventCreateWithFlags(&e, cudaEventDisableTiming); }
+  ~Event() { cudaEventDestroy(e); }
+};
+typedef std::shared_ptr<Event> EventRef;
+
 struct mav1cu_stream {
   drv::Norm n;
-  mav1cu_session *s;
+  mav1cu_session *eng[NUM_ENGINES];
+  uint8_t *staging[NUM_ENGINES];
   uint8_t *slot[8];
-  uint8_t *staging;
+  EventRef written[8];                // last write of each slot
+  std::vector<EventRef> readers[8];   // reference copies of the slot's picture since then
   size_t i420_bytes;
+  int last_engine;
 };
 
 extern "C" int mav1cu_stream_create(const mav1cu_config *cfg, mav1cu_stream **out, char *err, size_t errlen) {
@@ -612,20 +636,24 @@ extern "C" int mav1cu_stream_create(const mav1cu_config *cfg, mav1cu_stream **ou
     snprintf(err, errlen, "the device stream does not run the loop-restoration search (restoration must be 0)");
     return MAV1CU_ERR_ARG;
   }
-  mav1cu_session *s = NULL;
-  int rc = mav1cu_session_create(n.c.width, n.c.height, 4, &s, err, errlen);
-  if (rc) return rc;
   mav1cu_stream *st = new mav1cu_stream();
   st->n = n;
-  st->s = s;
-  size_t fb = s->g.frame_bytes;
+  for (int e = 0; e < NUM_ENGINES; e++) {
+    int rc = mav1cu_session_create(n.c.width, n.c.height, 4, &st->eng[e], err, errlen);
+    if (rc) {
+      mav1cu_stream_destroy(st);
+      return rc;
+    }
+  }
+  size_t fb = st->eng[0]->g.frame_bytes;
   st->i420_bytes = (size_t)n.c.width * n.c.height + 2 * (size_t)((n.c.width + 1) >> 1) * ((n.c.height + 1) >> 1);
   cudaError_t e = cudaSuccess;
   for (int k = 0; k < 8 && e == cudaSuccess; k++) {
     e = cudaMalloc(&st->slot[k], fb);
     if (e == cudaSuccess) e = cudaMemset(st->slot[k], 0, fb);
   }
-  if (e == cudaSuccess) e = cudaMalloc(&st->staging, st->i420_bytes);
+  for (int k = 0; k < NUM_ENGINES && e == cudaSuccess; k++) e = cudaMalloc(&st->staging[k], st->i420_bytes);
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
   if (e != cudaSuccess) {
     snprintf(err, errlen, "stream allocation failed: %s", cudaGetErrorString(e));
     mav1cu_stream_destroy(st);
@@ -637,16 +665,48 @@ extern "C" int mav1cu_stream_create(const mav1cu_config *cfg, mav1cu_stream **ou
 
 extern "C" void mav1cu_stream_destroy(mav1cu_stream *st) {
   if (!st) return;
-  if (st->s) cudaStreamSynchronize(st->s->stream);
-  for (int k = 0; k < 8; k++)
+  for (int e = 0; e < NUM_ENGINES; e++)
+    if (st->eng[e]) cudaStreamSynchronize(st->eng[e]->stream);
+  for (int k = 0; k < 8; k++) {
+    st->written[k].reset();
+    st->readers[k].clear();
     if (st->slot[k]) cudaFree(st->slot[k]);
-  if (st->staging) cudaFree(st->staging);
-  mav1cu_session_destroy(st->s);
+  }
+  for (int e = 0; e < NUM_ENGINES; e++) {
+    if (st->staging[e]) cudaFree(st->staging[e]);
+    mav1cu_session_destroy(st->eng[e]);
+  }
   delete st;
 }
 
-extern "C" mav1cu_session *mav1cu_stream_session(mav1cu_stream *st) { return st->s; }
+extern "C" mav1cu_session *mav1cu_stream_session(mav1cu_stream *st) { return st->eng[st->last_engine]; }
+extern "C" mav1cu_session *mav1cu_stream_engine(mav1cu_stream *st, int k) {
+  return k >= 0 && k < NUM_ENGINES ? st->eng[k] : NULL;
+}
+extern "C" int mav1cu_stream_engines(const mav1cu_stream *st) { return NUM_ENGINES; }
 extern "C" void *mav1cu_stream_slot(mav1cu_stream *st, int k) { return k >= 0 && k < 8 ? st->slot[k] : NULL; }
+
+// Orders work: every engine waits for `stream`'s work so far (wait) / `stream`
+// waits for every engine's work so far (join).
+extern "C" int mav1cu_stream_wait(mav1cu_stream *st, void *stream) {
+  Event ev;
+  cudaEventRecord(ev.e, (cudaStream_t)stream);
+  for (int k = 0; k < NUM_ENGINES; k++) cudaStreamWaitEvent(st->eng[k]->stream, ev.e, 0);
+  return check_cuda(st->eng[0], cudaGetLastError(), "stream wait");
+}
+extern "C" int mav1cu_stream_join(mav1cu_stream *st, void *stream) {
+  for (int k = 0; k < NUM_ENGINES; k++) {
+    Event ev;
+    cudaEventRecord(ev.e, st->eng[k]->stream);
+    cudaStreamWaitEvent((cudaStream_t)stream, ev.e, 0);
+  }
+  return check_cuda(st->eng[0], cudaGetLastError(), "stream join");
+}
+extern "C" int mav1cu_stream_synchronize(mav1cu_stream *st) {
+  for (int k = 0; k < NUM_ENGINES; k++)
+    if (mav1cu_synchronize(st->eng[k])) return st->eng[k]->err;
+  return MAV1CU_OK;
+}
 
 // Slots the reference encoder keeps (encoder.c:129-136): ALTREF driver 0, 2, 3
 // (and 4..7 with pyramid leaf frames); low-delay path LAST 0 and GOLDEN 1.
@@ -656,27 +716,38 @@ static int slot_exists(const drv::Norm &n, int k) {
 }
 
 extern "C" int mav1cu_stream_encode(mav1cu_stream *st, const mav1cu_frame_job *job, const void *i420, int on_device) {
-  mav1cu_session *s = st->s;
-  if (s->err) return s->err;
   const mav1cu_config &c = st->n.c;
+  int rf = job->is_key ? 0xFF : job->refresh;
+  int ei = rf ? 0 : 1;  // reference chain on engine 0, leaf frames on engine 1
+  mav1cu_session *s = st->eng[ei];
+  if (s->err) return s->err;
+  st->last_engine = ei;
   size_t fb = s->g.frame_bytes;
   const uint8_t *src = (const uint8_t *)i420;
   if (!on_device) {
-    if (check_cuda(s, cudaMemcpyAsync(st->staging, i420, st->i420_bytes, cudaMemcpyHostToDevice, s->stream), "source upload"))
+    if (check_cuda(s, cudaMemcpyAsync(st->staging[ei], i420, st->i420_bytes, cudaMemcpyHostToDevice, s->stream), "source upload"))
       return s->err;
-    src = st->staging;
+    src = st->staging[ei];
   }
   dim3 grid((s->g.stride[0] + 127) / 128, s->g.plane_h[0], 3);
   drv::k_load_source<<<grid, 128, 0, s->stream>>>(src, U8(s, MAV1CU_BUF_SRC), c.width, c.height, s->g.sb_cols,
                                                   s->g.sb_rows);
   if (after_launch(s, "load source")) return s->err;
   if (!job->is_key) {
-    if (job->last_slot < 0 || job->last_slot > 7) return set_error(s, MAV1CU_ERR_ARG, "stream: bad LAST slot");
-    if (check_cuda(s, cudaMemcpyAsync(s->buf[MAV1CU_BUF_REF], st->slot[job->last_slot], fb, cudaMemcpyDeviceToDevice, s->stream), "ref"))
-      return s->err;
-    if (job->arf_slot >= 0 &&
-        check_cuda(s, cudaMemcpyAsync(s->buf[MAV1CU_BUF_GOLD], st->slot[job->arf_slot], fb, cudaMemcpyDeviceToDevice, s->stream), "gold"))
-      return s->err;
+    int refs[2] = {job->last_slot, job->arf_slot};
+    int bufs[2] = {MAV1CU_BUF_REF, MAV1CU_BUF_GOLD};
+    for (int r = 0; r < 2; r++) {
+      int k = refs[r];
+      if (k < 0) continue;
+      if (k > 7) return set_error(s, MAV1CU_ERR_ARG, "stream: bad reference slot %d", k);
+      if (st->written[k]) cudaStreamWaitEvent(s->stream, st->written[k]->e, 0);
+      if (check_cuda(s, cudaMemcpyAsync(s->buf[bufs[r]], st->slot[k], fb, cudaMemcpyDeviceToDevice, s->stream), "reference copy"))
+        return s->err;
+    }
+    EventRef in = std::make_shared<Event>();
+    cudaEventRecord(in->e, s->stream);
+    for (int r = 0; r < 2; r++)
+      if (refs[r] >= 0) st->readers[refs[r]].push_back(in);
   }
   FrameParams fp;
   int presets = 0;
@@ -688,10 +759,22 @@ extern "C" int mav1cu_stream_encode(mav1cu_stream *st, const mav1cu_frame_job *j
   int filt = lfOn || (nPresets && !cdefOff) || !c.turbo;
   if (filt && (mav1cu_filter_info(s) || mav1cu_filter(s, presets))) return s->err;
   if (c.cdef && c.qindex > 0 && !cdefOff && mav1cu_cdef_select(s, nPresets)) return s->err;
-  int rf = job->is_key ? 0xFF : job->refresh;
-  for (int k = 0; k < 8; k++)
-    if (((rf >> k) & 1) && slot_exists(st->n, k) &&
-        check_cuda(s, cudaMemcpyAsync(st->slot[k], s->buf[MAV1CU_BUF_REC], fb, cudaMemcpyDeviceToDevice, s->stream), "slot"))
+  EventRef out;
+  for (int k = 0; k < 8; k++) {
+    if (!((rf >> k) & 1) || !slot_exists(st->n, k)) continue;
+    for (auto &r : st->readers[k]) cudaStreamWaitEvent(s->stream, r->e, 0);
+    if (st->written[k]) cudaStreamWaitEvent(s->stream, st->written[k]->e, 0);
+    if (check_cuda(s, cudaMemcpyAsync(st->slot[k], s->buf[MAV1CU_BUF_REC], fb, cudaMemcpyDeviceToDevice, s->stream), "slot"))
       return s->err;
-  return MAV1CU_OK;
+  }
+  if (rf) {
+    out = std::make_shared<Event>();
+    cudaEventRecord(out->e, s->stream);
+    for (int k = 0; k < 8; k++)
+      if (((rf >> k) & 1) && slot_exists(st->n, k)) {
+        st->written[k] = out;
+        st->readers[k].clear();
+      }
+  }
+  return check_cuda(s, cudaGetLastError(), "stream encode");
 }

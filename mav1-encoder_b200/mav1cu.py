@@ -62,7 +62,8 @@ EXPORTS = [
     "mav1cu_filter_info", "mav1cu_filter", "mav1cu_cdef_select", "mav1cu_restore", "mav1cu_synchronize",
     "mav1cu_error_string", "mav1cu_launch_count", "mav1cu_build_fwd_matrices", "mav1cu_plan",
     "mav1cu_frame_params_for", "mav1cu_stream_create", "mav1cu_stream_destroy", "mav1cu_stream_session",
-    "mav1cu_stream_encode", "mav1cu_stream_slot",
+    "mav1cu_stream_encode", "mav1cu_stream_slot", "mav1cu_stream_engines", "mav1cu_stream_engine",
+    "mav1cu_stream_wait", "mav1cu_stream_join", "mav1cu_stream_synchronize",
 ]
 
 
@@ -114,6 +115,15 @@ def load_library(path=LIB_PATH):
     lib.mav1cu_stream_encode.restype = i32
     lib.mav1cu_stream_slot.argtypes = [vp, i32]
     lib.mav1cu_stream_slot.restype = vp
+    lib.mav1cu_stream_engines.argtypes = [vp]
+    lib.mav1cu_stream_engines.restype = i32
+    lib.mav1cu_stream_engine.argtypes = [vp, i32]
+    lib.mav1cu_stream_engine.restype = vp
+    for f in ("mav1cu_stream_wait", "mav1cu_stream_join"):
+        getattr(lib, f).argtypes = [vp, vp]
+        getattr(lib, f).restype = i32
+    lib.mav1cu_stream_synchronize.argtypes = [vp]
+    lib.mav1cu_stream_synchronize.restype = i32
     return lib
 
 
@@ -279,9 +289,20 @@ def frame_params(cfg, job):
     return fp, presets.value
 
 
+class _EngineSession(Session):
+    """A session owned by a stream (not closed by Python)."""
+
+    def __init__(self, lib_, ptr, geom):
+        self.lib, self.h, self.geom = lib_, ctypes.c_void_p(ptr), geom
+
+    def close(self):
+        pass
+
+
 class Stream:
     """Device-resident stream (mav1cu_stream): planned frames coded through
-    every device stage with the reference slots in HBM."""
+    every device stage with the reference slots in HBM, reference-chain and
+    non-reference frames on two concurrent engines."""
 
     def __init__(self, cfg):
         self.lib = lib()
@@ -292,17 +313,39 @@ class Stream:
         if rc:
             raise Mav1cuError(f"mav1cu_stream_create: {err.value.decode()} ({rc})")
         self.h = h
-        self.session = Session.__new__(Session)
-        self.session.lib = self.lib
-        self.session.geom = geometry(int(cfg[0]["width"]), int(cfg[0]["height"]))
-        self.session.h = ctypes.c_void_p(self.lib.mav1cu_stream_session(h))
-        self.session.close = lambda: None
+        geom = geometry(int(cfg[0]["width"]), int(cfg[0]["height"]))
+        self.engines = [_EngineSession(self.lib, self.lib.mav1cu_stream_engine(h, k), geom)
+                        for k in range(self.lib.mav1cu_stream_engines(h))]
+        self.session = self.engines[0]
+
+    @staticmethod
+    def engine_of(job):
+        """Engine that codes the job: 0 for frames that refresh a slot, else 1."""
+        return 0 if (job["is_key"] or job["refresh"]) else 1
 
     def encode(self, job, i420_ptr, on_device):
+        """Enqueues one planned frame; returns the session holding its outputs."""
         j = np.array([job], JOB_DTYPE)
         rc = self.lib.mav1cu_stream_encode(self.h, j.ctypes.data, i420_ptr, 1 if on_device else 0)
+        e = self.engines[self.engine_of(job)]
         if rc:
-            raise Mav1cuError(f"mav1cu_stream_encode: {self.lib.mav1cu_error_string(self.session.h).decode()}")
+            raise Mav1cuError(f"mav1cu_stream_encode: {self.lib.mav1cu_error_string(e.h).decode()}")
+        return e
+
+    def wait(self, cuda_stream):
+        self.lib.mav1cu_stream_wait(self.h, cuda_stream)
+
+    def join(self, cuda_stream):
+        self.lib.mav1cu_stream_join(self.h, cuda_stream)
+
+    def synchronize(self):
+        rc = self.lib.mav1cu_stream_synchronize(self.h)
+        if rc:
+            msgs = [self.lib.mav1cu_error_string(e.h).decode() for e in self.engines]
+            raise Mav1cuError(f"stream: {msgs}")
+
+    def launches(self):
+        return sum(e.launches() for e in self.engines)
 
     def slot_ptr(self, k):
         return self.lib.mav1cu_stream_slot(self.h, k)

@@ -252,3 +252,127 @@ def check_all(sess, tr, cfg, stages=STAGES):
         fc = FrameCheck(sess, tr, cfg, fr)
         res.append((k, fr["state"], {st: getattr(fc, st)() for st in stages}))
     return res
+
+
+# ---- whole-stream comparisons -------------------------------------------------------
+import os
+import re
+
+_TABLES = None
+
+
+def spec_tables():
+    """The normative tables the library is compiled with (csrc/spec_tables_gen.h)."""
+    global _TABLES
+    if _TABLES is None:
+        path = os.path.join(os.path.dirname(mav1cu.__file__), "csrc", "spec_tables_gen.h")
+        text = open(path).read()
+        _TABLES = {}
+        for name, dims, body in re.findall(r"#define MAV1T_(\w+)_DIMS ((?:\[\d+\])+)\n#define MAV1T_\1 \{(.*?)\}", text, re.S):
+            shape = [int(d) for d in re.findall(r"\d+", dims)]
+            vals = [int(v) for v in re.findall(r"-?\d+", body.replace("\\", " "))]
+            _TABLES[name] = np.array(vals, np.int64).reshape(shape)
+    return _TABLES
+
+
+def tx_layout(b, plane, p):
+    """(txSz, [(startX, startY)]) of the transform blocks code_plane codes for
+    plane `plane` of block b (k_recon.h:190-291)."""
+    T = spec_tables()
+    bs = int(b["bsize"])
+    sub = 1 if plane else 0
+    if p["lossless"]:
+        tx = 0
+    elif plane:
+        uv = int(T["Max_Tx_Size_Rect"][T["Subsampled_Size"][bs][1][1]])
+        tw, th = T["Tx_Width"][uv], T["Tx_Height"][uv]
+        tx = uv
+        if tw == 64 or th == 64:
+            tx = 9 if tw == 16 else 10 if th == 16 else 3
+    else:
+        tx = int(T["Max_Tx_Size_Rect"][bs])
+        for _ in range(int(b["tx_depth"]) if not b["is_inter"] else 0):
+            tx = int(T["Split_Tx_Size"][tx])
+    psz = int(T["Subsampled_Size"][bs][sub][sub])
+    n4w, n4h = int(T["Num_4x4_Blocks_Wide"][psz]), int(T["Num_4x4_Blocks_High"][psz])
+    bx, by = (int(b["mi_col"]) >> sub) * 4, (int(b["mi_row"]) >> sub) * 4
+    sx, sy = int(T["Tx_Width"][tx]) >> 2, int(T["Tx_Height"][tx]) >> 2
+    starts = []
+    for y in range(0, n4h, sy):
+        for x in range(0, n4w, sx):
+            X, Y = bx + 4 * x, by + 4 * y
+            if X >= (p["mi_cols"] * 4) >> sub or Y >= (p["mi_rows"] * 4) >> sub:
+                continue
+            starts.append((X, Y))
+    return tx, starts
+
+
+def used_coefs(blocks, sbs, p):
+    """Indices of the coefficient buffer the frame's blocks write."""
+    T = spec_tables()
+    idx = []
+    for r in sbs:
+        for b in blocks[r["first_block"]: r["first_block"] + r["num_blocks"]]:
+            for plane in range(3):
+                tx, starts = tx_layout(b, plane, p)
+                w, h = int(T["Tx_Width"][tx]), int(T["Tx_Height"][tx])
+                n = min(32, w) * min(32, h)
+                for k in range(len(starts)):
+                    o = int(b["coef_off"][plane]) + k * w * h
+                    idx.append(np.arange(o, o + n))
+    return np.concatenate(idx) if idx else np.zeros(0, np.int64)
+
+
+def visible(frame, g):
+    """The frame's displayed samples (w x h luma, (w+1)/2 x (h+1)/2 chroma) from a padded buffer."""
+    w, h = g["w"], g["h"]
+    s0, s1 = g["stride"][0], g["stride"][1]
+    o1, o2 = g["offset"][1], g["offset"][2]
+    cw, ch = (w + 1) // 2, (h + 1) // 2
+    y = frame[: s0 * g["plane_h"][0]].reshape(-1, s0)[:h, :w]
+    u = frame[o1: o1 + s1 * g["plane_h"][1]].reshape(-1, s1)[:ch, :cw]
+    v = frame[o2: o2 + s1 * g["plane_h"][2]].reshape(-1, s1)[:ch, :cw]
+    return np.concatenate([y.ravel(), u.ravel(), v.ravel()])
+
+
+def stream_vs_oracle(tr, frames, flags, spec):
+    """Codes the traced clip through the device stream (mav1cu_stream, both
+    engines) and compares every frame's writer inputs and reconstruction with
+    the oracle's, in coding order. Returns [(frame, {output: mismatches})]."""
+    cfg = mav1cu.cli_config(spec.width, spec.height, **flags)
+    jobs = mav1cu.plan(cfg, len(frames))
+    assert len(jobs) == len(tr.frames)
+    st = mav1cu.Stream(cfg)
+    g = mav1cu.geometry(spec.width, spec.height)
+    dev = [np.ascontiguousarray(np.frombuffer(synthetic.packed(f), np.uint8)) for f in frames]
+    import torch
+    dframes = [torch.from_numpy(d).cuda() for d in dev]
+    res = []
+    try:
+        for k, (job, fr) in enumerate(zip(jobs, tr.frames)):
+            sess = st.encode(job, dframes[job["disp"]].data_ptr(), True)
+            st.synchronize()
+            p = params_of(fr).view(PARAMS_DTYPE)[0]
+            fb = g["frame_bytes"]
+            out = {}
+            rec = sess.download("REC", count=fb)
+            done = fr[(ST["DONE"], "REC")][:fb]
+            out["rec"] = int((visible(rec, g) != visible(done, g)).sum())
+            blocks = sess.download("BLOCKS", count=sess.size("BLOCKS")).view(BLOCK_DTYPE)
+            sbs = sess.download("SBS", count=sess.size("SBS")).view(SB_DTYPE)
+            rb = fr[(ST["RECON"], "BLOCKS")][: sess.size("BLOCKS")].view(BLOCK_DTYPE)
+            rs = fr[(ST["ANALYZE"], "SBS")][: sess.size("SBS")].view(SB_DTYPE)
+            out["sbs"] = int((sbs != rs).sum())
+            sel = np.concatenate([np.arange(r["first_block"], r["first_block"] + r["num_blocks"]) for r in rs])
+            out["blocks"] = blocks_diff(blocks[sel], rb[sel])
+            coefs = sess.download("COEFS", np.int32)
+            rcoefs = fr[(ST["RECON"], "COEFS")][: sess.size("COEFS")].view(np.int32)
+            used = used_coefs(rb, rs, p)
+            out["coefs"] = int((coefs[used] != rcoefs[used]).sum())
+            if (ST["CDEFSEL"], "CDEF_CHOICE") in fr and fr["state"]["leafopt"] & 4 == 0:
+                n = g["num_sbs"]
+                out["cdef_choice"] = int((sess.download("CDEF_CHOICE", count=n) != fr[(ST["CDEFSEL"], "CDEF_CHOICE")][:n]).sum())
+            res.append((k, out))
+    finally:
+        st.close()
+    return res
