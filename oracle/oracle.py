@@ -16,6 +16,8 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_ref", "libmav1ref.so")
+# the same driver built with the CUDA backend (backend_cuda.c) behind the vtable
+HYB_PATH = os.path.join(HERE, "_ref", "libmav1hyb.so")
 
 STAGE = dict(PARAMS=0, ME=1, ANALYZE=2, EDGE=3, RECON=4, FINFO=5, FILTER=6, CDEFSEL=7, LRSEL=8, RESTORE=9, DONE=10)
 OBUF = dict(SRC=0, REC=1, REF=2, GOLD=3, PARAMS=4, MATS=5, MVFIELD=6, MVGOLD=7, BLOCKS=8, SBS=9, COEFS=10,
@@ -32,19 +34,18 @@ class Mav1Config(ctypes.Structure):
 
 HOOK = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p)
 
-_lib = None
+_libs = {}
 
 
-def available():
-    return os.path.exists(LIB_PATH)
+def available(path=LIB_PATH):
+    return os.path.exists(path)
 
 
-def lib():
-    global _lib
-    if _lib is None:
-        if not available():
-            raise RuntimeError(f"oracle not built ({LIB_PATH}); run make -C oracle")
-        L = ctypes.CDLL(LIB_PATH)
+def lib(path=LIB_PATH):
+    if path not in _libs:
+        if not available(path):
+            raise RuntimeError(f"oracle not built ({path}); run make -C oracle")
+        L = ctypes.CDLL(path)
         vp = ctypes.c_void_p
         L.mav1_default_config.argtypes = [ctypes.POINTER(Mav1Config), ctypes.c_int, ctypes.c_int]
         L.mav1_create.argtypes = [ctypes.POINTER(Mav1Config), ctypes.c_char_p, ctypes.c_size_t]
@@ -62,15 +63,15 @@ def lib():
         L.oref_struct_sizes.argtypes = [ctypes.POINTER(ctypes.c_int32)]
         L.oref_run_stage.argtypes = [vp, ctypes.c_int]
         L.oref_set_num_cdef_presets.argtypes = [vp, ctypes.c_int]
-        _lib = L
-    return _lib
+        _libs[path] = L
+    return _libs[path]
 
 
-def cli_config(width, height, q=100, cpu=True, keyint=0, lf=1, cdef=1, txs=1, txd=1, lr=1, lr_test=0, sw=1,
+def cli_config(width, height, q=100, cpu=True, path=LIB_PATH, keyint=0, lf=1, cdef=1, txs=1, txd=1, lr=1, lr_test=0, sw=1,
                fast=0, turbo=0, golden=0, altref=0, leaf=0, edge=1, tiles=-1, me_range=32):
     """Mav1Config exactly as tools/mav1enc.c:36-104 builds it from its flags."""
     cfg = Mav1Config()
-    lib().mav1_default_config(ctypes.byref(cfg), width, height)
+    lib(path).mav1_default_config(ctypes.byref(cfg), width, height)
     if turbo:
         fast = 1
     cfg.qindex = q
@@ -180,11 +181,14 @@ def _planes(frame, w, h):
     return arrs, ptrs, strides
 
 
-def encode(frames, cfg, trace=None, factory=None):
+def encode(frames, cfg, trace=None, factory=None, path=LIB_PATH):
     """Encodes the frames through mav1_send_frame / mav1_receive_packet like
     tools/mav1enc.c. Returns (packets, recons): the temporal units and the
-    shown reconstruction of each (I420 planes)."""
-    L = lib()
+    shown reconstruction of each (I420 planes). With path=HYB_PATH and
+    cuda=True in cfg.use_metal the CUDA backend codes every frame."""
+    L = lib(path)
+    if factory == "cuda":
+        factory = ctypes.cast(L.backend_cuda_create, ctypes.c_void_p)
     L.oref_set_hook(trace.cb if trace else HOOK(), None)
     L.oref_set_backend_factory(factory)
     err = ctypes.create_string_buffer(256)

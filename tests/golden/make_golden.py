@@ -1,0 +1,55 @@
+#!/usr/bin/env python3
+"""Writes tests/golden/oracle_hashes.json: SHA-256 of the oracle's output
+(IVF bitstream, shown reconstructions, MAV1_DUMP_DEC decision dump) for
+seeded synthetic clips, plus the hash of the clips themselves. Run on a
+machine with the oracle built (make -C oracle); the fixture pins the oracle
+(the reference's scalar CPU path) so later runs detect any change in it."""
+import hashlib
+import json
+import os
+import sys
+import tempfile
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path[:0] = [os.path.join(ROOT, "mav1-encoder_b200"), os.path.join(ROOT, "oracle")]
+
+import oracle  # noqa: E402
+import synthetic  # noqa: E402
+
+CASES = {
+    "c0_turbo_q125": (dict(width=352, height=288, frames=30, seed=1), dict(q=125, turbo=1, keyint=30, tiles=0)),
+    "full_203x131": (dict(width=203, height=131, frames=9, seed=41, rects=3, rect_size=(16, 48)),
+                     dict(q=90, altref=4, golden=1, tiles=1, me_range=64)),
+    "lowdelay_lr_150x102": (dict(width=150, height=102, frames=6, seed=42, rects=2, rect_size=(16, 40)),
+                            dict(q=200, golden=1, keyint=4, lr_test=1)),
+    "lossless_96x64": (dict(width=96, height=64, frames=3, seed=43, rects=1, rect_size=(16, 32)), dict(q=0, fast=1)),
+}
+
+
+def run(name):
+    spec_kw, flags = CASES[name]
+    spec = synthetic.ClipSpec(**spec_kw)
+    frames = list(synthetic.generate(spec))
+    with tempfile.TemporaryDirectory() as d:
+        dump = os.path.join(d, "dec")
+        os.environ["MAV1_DUMP_DEC"] = dump
+        try:
+            packets, recons = oracle.encode(frames, oracle.cli_config(spec.width, spec.height, **flags))
+        finally:
+            del os.environ["MAV1_DUMP_DEC"]
+        dec = open(dump, "rb").read()
+    h = lambda b: hashlib.sha256(b).hexdigest()
+    return {
+        "clip": synthetic.clip_sha256(spec),
+        "ivf": h(oracle.ivf_bytes(packets, spec.width, spec.height)),
+        "recon": h(b"".join(p.tobytes() for r in recons for p in r)),
+        "dump": h(dec),
+        "packets": len(packets),
+    }
+
+
+if __name__ == "__main__":
+    out = {name: run(name) for name in CASES}
+    json.dump(out, open(os.path.join(HERE, "oracle_hashes.json"), "w"), indent=1, sort_keys=True)
+    print(json.dumps(out, indent=1))

@@ -1,0 +1,51 @@
+"""The drop-in: the encoder's own driver, tile writer and LR search with the
+CUDA backend behind the unchanged Backend vtable (backend_cuda.c over
+libmav1cu) against the same driver with the reference CPU backend. The IVF
+bitstreams, the reconstructions returned by mav1_get_recon and the
+MAV1_DUMP_DEC decision dumps must be byte-identical."""
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+import synthetic
+
+pytestmark = pytest.mark.gpu
+
+CASES = {
+    "c0_turbo": (synthetic.CONFIGS["c0_352x288"], 13, dict(q=125, turbo=1, keyint=30, tiles=0)),
+    "full_tools": (synthetic.ClipSpec(203, 131, 7, seed=31, rects=3, rect_size=(16, 48)), 7,
+                   dict(q=90, altref=4, golden=1, tiles=1, me_range=64)),
+    "lowdelay_lr": (synthetic.ClipSpec(150, 102, 5, seed=32, rects=2, rect_size=(16, 40)), 5,
+                    dict(q=200, golden=1, keyint=4, lr_test=1)),
+    "lossless": (synthetic.ClipSpec(96, 64, 3, seed=33, rects=1, rect_size=(16, 32)), 3, dict(q=0, fast=1)),
+}
+
+
+def _encode(spec, n, flags, cuda, dump):
+    frames = list(synthetic.generate(spec, n))
+    os.environ["MAV1_DUMP_DEC"] = dump
+    try:
+        path = oracle.HYB_PATH if cuda else oracle.LIB_PATH
+        cfg = oracle.cli_config(spec.width, spec.height, cpu=not cuda, **flags)
+        cfg_lib = oracle.lib(path)
+        return oracle.encode(frames, cfg, factory="cuda" if cuda else None, path=path)
+    finally:
+        del os.environ["MAV1_DUMP_DEC"]
+
+
+@pytest.mark.skipif(not (oracle.available() and oracle.available(oracle.HYB_PATH)), reason="oracle not built")
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_dropin_bitstream_identical(name, tmp_path):
+    spec, n, flags = CASES[name]
+    pk_cpu, rec_cpu = _encode(spec, n, flags, False, str(tmp_path / "cpu.dec"))
+    pk_gpu, rec_gpu = _encode(spec, n, flags, True, str(tmp_path / "cuda.dec"))
+    ivf_cpu = oracle.ivf_bytes(pk_cpu, spec.width, spec.height)
+    ivf_gpu = oracle.ivf_bytes(pk_gpu, spec.width, spec.height)
+    assert len(pk_cpu) == len(pk_gpu)
+    assert ivf_cpu == ivf_gpu, [i for i, (a, b) in enumerate(zip(pk_cpu, pk_gpu)) if a != b]
+    for a, b in zip(rec_cpu, rec_gpu):
+        for pa, pb in zip(a, b):
+            assert np.array_equal(pa, pb)
+    assert (tmp_path / "cpu.dec").read_bytes() == (tmp_path / "cuda.dec").read_bytes()
