@@ -298,6 +298,27 @@ int mav1cu_stream_synchronize(mav1cu_stream *st);
  * (fwd_matrices.c:17-65). */
 void mav1cu_build_fwd_matrices(int32_t *mats);
 
+/* ---- edge types without allocation ---------------------------------------- */
+/* No counterpart in the reference. The result of mav1cu_edge_types
+ * (interp_filter bits 4/5 of every block) on caller-owned device buffers,
+ * enqueued on `stream` (a cudaStream_t; NULL is the legacy default stream),
+ * without allocating device memory: for hosts that fix their device memory
+ * at start-up or whose other streams must not be stalled by cudaMalloc /
+ * cudaFree. `params` is a device copy of the frame's mav1cu_frame_params;
+ * `blocks` / `sbs` are the analysis output (num_sbs superblocks);
+ * mi_rows / mi_cols are the frame's size in 4x4 units and must match params.
+ * Scratch is a fixed device array of 2 x 1,048,576 bytes per device: frames
+ * above 1,048,576 4x4 units (4096 x 4096 luma samples) are refused with
+ * MAV1CU_ERR_ARG. Each call clears the scratch it uses first. Calls that
+ * overlap in time on one device share that scratch and race: order them on
+ * one stream or with events. The first call on each device looks up the
+ * scratch address (it may load the device code): make it before any stream
+ * capture on that device. Returns MAV1CU_OK once the work is enqueued;
+ * errors are written to err. */
+int mav1cu_edge_types_noalloc(const mav1cu_frame_params *params, mav1cu_block_info *blocks,
+                              const mav1cu_sb_info *sbs, int mi_rows, int mi_cols, int num_sbs, void *stream,
+                              char *err, size_t errlen);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,7 +1,9 @@
 """Builds libmav1cu.so (the sm_100a kernels and their C ABI) in-tree.
 
-nvcc compiles the single translation unit csrc/session.cu for
-compute_100a / sm_100a with line info; host code is compiled without
+nvcc compiles the translation units csrc/session.cu (the session and stream
+API over every stage) and csrc/edge_noalloc.cu (the entry point that
+allocates nothing) for compute_100a / sm_100a with line info; host code is
+compiled without
 floating-point contraction (the forward-matrix derivation must round like
 the reference's). The library lands next to this file so it travels with
 the working tree.
@@ -41,7 +43,7 @@ def build(force=False, verbose=False, extra=()):
     if not force and not stale(LIB, deps):
         return LIB
     cmd = [NVCC, *NVCC_FLAGS, *extra, "-I", os.path.join(ROOT, "include"), "-I", CSRC,
-           os.path.join(CSRC, "session.cu"), "-o", LIB + ".tmp"]
+           os.path.join(CSRC, "session.cu"), os.path.join(CSRC, "edge_noalloc.cu"), "-o", LIB + ".tmp"]
     if verbose:
         print(" ".join(cmd), file=sys.stderr)
     r = subprocess.run(cmd, capture_output=True, text=True)

@@ -63,7 +63,7 @@ EXPORTS = [
     "mav1cu_error_string", "mav1cu_launch_count", "mav1cu_build_fwd_matrices", "mav1cu_plan",
     "mav1cu_frame_params_for", "mav1cu_stream_create", "mav1cu_stream_destroy", "mav1cu_stream_session",
     "mav1cu_stream_encode", "mav1cu_stream_slot", "mav1cu_stream_engines", "mav1cu_stream_engine",
-    "mav1cu_stream_wait", "mav1cu_stream_join", "mav1cu_stream_synchronize",
+    "mav1cu_stream_wait", "mav1cu_stream_join", "mav1cu_stream_synchronize", "mav1cu_edge_types_noalloc",
 ]
 
 
@@ -124,6 +124,8 @@ def load_library(path=LIB_PATH):
         getattr(lib, f).restype = i32
     lib.mav1cu_stream_synchronize.argtypes = [vp]
     lib.mav1cu_stream_synchronize.restype = i32
+    lib.mav1cu_edge_types_noalloc.argtypes = [vp, vp, vp, i32, i32, i32, vp, ctypes.c_char_p, sz]
+    lib.mav1cu_edge_types_noalloc.restype = i32
     return lib
 
 
