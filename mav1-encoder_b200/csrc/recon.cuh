@@ -8,21 +8,25 @@
 // the normative inverse transform added back into `rec`; optional luma
 // transform-type search and intra tx_depth search by 16 * SSE + lambda * bits.
 //
-// B200 mapping. An inter block's prediction reads only reference pictures,
-// so every inter block of the frame is coded in one launch (phase 0: one
-// CTA per superblock, all superblocks at once). Intra blocks read their
-// reconstructed neighbours: a superblock's intra blocks may start once its
-// left and above-right neighbours in its tile column are complete, the
-// reference's dependency (backend_cpu.c:76-86). Phase 1 is one persistent
-// launch whose CTAs claim superblocks in wave order ((c - tileStart) + 2r)
-// and wait on per-superblock completion flags, so a superblock without
-// intra blocks costs nothing and unrelated chains proceed independently;
-// inside a superblock the blocks run in decode order and the inter blocks
-// only mark their BlockDecoded flags. Samples of the frame being written
-// are read through L2 (ldpx), as other CTAs write them during the launch. Within a transform block
-// the CTA's 256 threads split the residual, both matrix passes (64-bit
-// accumulation), the quantiser, the eob search (a max over inverse-scan
-// positions), the row / column inverse kernels and the reconstruction.
+// B200 mapping: one launch per frame codes every block, one warp (a CTA of
+// 32 threads) per block. Blocks are claimed from a list in superblock wave
+// order ((c - tileStart) + 2r), decode order inside a superblock: a
+// topological order of the sample dependencies, so a persistent worker that
+// waits only ever waits on blocks already claimed by running workers. An
+// inter block reads reference pictures only and starts at once. Before
+// each intra transform block the worker waits on the completion flags of
+// exactly the blocks whose samples its edges read (above row to the
+// aboveLimit, left column to the leftLimit, spec 7.11.2), so the critical
+// path follows the block-level wavefront instead of whole superblocks.
+// BlockDecoded availability is a function of the decode order: a unit of
+// the superblock is decoded when the block covering it precedes this one
+// (a map from 4x4 units to block indices), or by the clear-flags rule
+// (k_recon.h:402-414) outside the superblock. Samples of the frame being
+// written are read through L2 (ldpx), as other SMs write them during the
+// launch. Within a transform block the warp splits the residual, both
+// matrix passes (64-bit accumulation), the quantiser, the eob search (a max
+// over inverse-scan positions), the row / column inverse kernels and the
+// reconstruction.
 #pragma once
 
 #include "common.cuh"
@@ -31,8 +35,7 @@
 
 namespace rec {
 
-#define RT 256  // threads per CTA
-#define BD_DIM 18
+#define RT 32  // threads per CTA: one warp, one block worker
 #define FWD_SLOT_SIZE 4096
 HD int fwd_slot(int kind, int log2n) { return (kind * 5 + log2n - 2) * FWD_SLOT_SIZE; }
 
@@ -55,15 +58,10 @@ struct Ctx {
   const SbInfo *sbs;
   int32_t *coefs;
   const int32_t *mats;
-  int *status;
+  int *status;          // [0] error code, [1] abort
+  const int *blk_at;    // per 4x4 luma unit of the frame: index of the block covering it
+  int *done;            // per block index: 1 once its samples are written
 };
-
-#define TILE_Y_W 129  // luma tile: x in [-1, 128), y in [-1, 64) relative to the superblock
-#define TILE_Y_H 65
-#define TILE_C_W 65   // chroma tile: x in [-1, 64), y in [-1, 32)
-#define TILE_C_H 33
-#define TILE_Y_BYTES (TILE_Y_W * TILE_Y_H)
-#define TILE_C_BYTES (TILE_C_W * TILE_C_H)
 
 struct Smem {
   int32_t resid[64 * 64];  // residual, then the inverse transform's plane
@@ -71,44 +69,33 @@ struct Smem {
   int32_t q[32 * 32];      // levels of the current candidate
   int32_t qbest[32 * 32];  // levels kept by the tx type search
   int edge[3][EDGE_LEN];   // AboveRow, LeftCol, filter copy
-  uint8_t bd[3 * BD_DIM * BD_DIM];
-  uint8_t bdsave[BD_DIM * BD_DIM];
   uint8_t save[64 * 64];
-  long long red[RT / 32 + 1];
   int sse33[33];
   BlockInfo blk;
   int maxLumaW, maxLumaH;
   int flag;
-  // views of the reconstruction: plane origins (absolute plane coordinates)
-  // and strides; the global frame in phase 0, the superblock tile below in
-  // phase 1
+  int me;      // index of the block being coded
+  int r0, c0;  // its superblock's first 4x4 row / column
+  // the reconstruction: plane origins (absolute plane coordinates), strides
   uint8_t *recp[3];
   int rstride[3];
-  // phase 1: the superblock's samples with a one-sample top / left halo and
-  // the above row extended over the above-right superblock
-  uint8_t tile[TILE_Y_BYTES + 2 * TILE_C_BYTES];
 };
 
-#define BD(sm, p, y, x) (sm).bd[(p) * BD_DIM * BD_DIM + ((y) + 1) * BD_DIM + ((x) + 1)]
-
-__device__ __forceinline__ long long cta_sum64(long long v, Smem &sm) {
+// Sums / maxima over the worker (one warp); the __syncwarp()s order the
+// shared-memory writes before and after like a block barrier would.
+__device__ __forceinline__ long long cta_sum64(long long v, Smem &) {
+  __syncwarp();
   for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
-  if ((threadIdx.x & 31) == 0) sm.red[threadIdx.x >> 5] = v;
-  __syncthreads();
-  long long s = 0;
-  for (int k = 0; k < RT / 32; k++) s += sm.red[k];
-  __syncthreads();
-  return s;
+  __syncwarp();
+  return v;
 }
-__device__ __forceinline__ int cta_max(int v, Smem &sm) {
+__device__ __forceinline__ int cta_max(int v, Smem &) {
+  __syncwarp();
   for (int off = 16; off > 0; off >>= 1) v = imax(v, __shfl_xor_sync(0xffffffffu, v, off));
-  if ((threadIdx.x & 31) == 0) sm.red[threadIdx.x >> 5] = v;
-  __syncthreads();
-  int m = 0;
-  for (int k = 0; k < RT / 32; k++) m = imax(m, (int)sm.red[k]);
-  __syncthreads();
-  return m;
+  __syncwarp();
+  return v;
 }
+static_assert(RT == 32, "the worker reductions assume one warp per CTA");
 
 struct CtaSync {
   __device__ void operator()() const { __syncthreads(); }
@@ -367,7 +354,7 @@ __device__ int cfl_alpha(Smem &sm, const uint8_t *luma, int ls, int startX, int 
       sse[a] += d * d;
     }
   }
-  if (threadIdx.x < 33) sm.sse33[threadIdx.x] = 0;
+  for (int a = threadIdx.x; a < 33; a += RT) sm.sse33[a] = 0;
   __syncthreads();
   for (int a = 0; a < 33; a++) {
     int v = sse[a];
@@ -390,6 +377,75 @@ __device__ int cfl_alpha(Smem &sm, const uint8_t *luma, int ls, int startX, int 
   return bestA;
 }
 
+// BlockDecoded[plane][y][x] (superblock-relative units of the plane, -1..n)
+// as the reference's flags hold it when block sm.me codes a transform
+// block: outside the superblock, clear_block_decoded_flags' values
+// (k_recon.h:402-414); inside, set by every block before this one in decode
+// order. `own` answers for a unit of this block itself: its transform blocks
+// run in raster order, so the unit above-right of one is coded (1) and the
+// unit below-left is not (0). Units beyond the frame report 0: the edge
+// limits clip to maxX / maxY there, so their flag is never used.
+__device__ int decoded(const Ctx &c, const Smem &sm, int plane, int y, int x, int own) {
+  const FrameParams *fp = c.fp;
+  int sub = plane > 0, n = 16 >> sub;
+  if (y < 0 || x < 0 || y >= n || x >= n) {
+    if (y == n && x == -1) return 0;
+    if (y < 0) return x < ((tile_col_end(fp, sm.c0) - sm.c0) >> sub);
+    if (x < 0) return y < ((fp->mi_rows - sm.r0) >> sub);
+    return 0;
+  }
+  int r = sm.r0 + (y << sub), col = sm.c0 + (x << sub);
+  if (r >= fp->mi_rows || col >= fp->mi_cols) return 0;
+  int b = c.blk_at[r * fp->mi_cols + col];
+  return b == sm.me ? own : (b >= 0 && b < sm.me);
+}
+
+#define SPIN_LIMIT (1 << 22)  // polls of at least one L2 round trip each: about a second
+
+// Waits until every other block whose samples intra_edges reads for this
+// transform block is complete: the above row from the corner (or x) to the
+// above limit, the left column from the corner (or y) to the left limit.
+// Each lane polls the completion flag of the block covering one 4x4 unit.
+// The blocks waited on precede this one in the claim order, so the wait
+// ends; past the limit it sets the error and abort words and gives up, and
+// every other wait then stops too.
+__device__ void wait_edges(const Ctx &c, Smem &sm, int plane, const pred::IntraArgs &a, int x, int y) {
+  const FrameParams *fp = c.fp;
+  int sub = plane > 0, w = 1 << a.log2W, h = 1 << a.log2H;
+  int nA = 0, nL = 0, rowA = 0, colA0 = 0, colL = 0, rowL0 = 0;
+  if (a.haveAbove) {
+    int lim = imin(imin(a.maxX, x + (a.haveAboveRight ? 2 * w : w) - 1), x + w + h - 1);
+    rowA = ((y - 1) << sub) >> 2;
+    colA0 = ((a.haveLeft ? x - 1 : x) << sub) >> 2;
+    nA = ((lim << sub) >> 2) - colA0 + 1;
+  }
+  if (a.haveLeft) {
+    int lim = imin(imin(a.maxY, y + (a.haveBelowLeft ? 2 * h : h) - 1), y + w + h - 1);
+    colL = ((x - 1) << sub) >> 2;
+    rowL0 = ((a.haveAbove ? y - 1 : y) << sub) >> 2;
+    nL = ((lim << sub) >> 2) - rowL0 + 1;
+  }
+  volatile const int *vdone = c.done;
+  volatile int *vstatus = c.status;
+  for (int i = threadIdx.x; i < nA + nL; i += RT) {
+    int r = i < nA ? rowA : rowL0 + (i - nA), col = i < nA ? colA0 + i : colL;
+    int b = c.blk_at[r * fp->mi_cols + col];
+    if (b == sm.me || (unsigned)b >= (unsigned)(fp->sb_cols * fp->sb_rows * MAX_BLOCKS_PER_SB)) continue;
+    int spins = 0;
+    while (!vdone[b]) {
+      if (vstatus[1] || ++spins > SPIN_LIMIT) {
+        if (!vstatus[1]) {
+          atomicExch(c.status, 1);
+          atomicExch(c.status + 1, 1);
+        }
+        break;
+      }
+      __nanosleep(64);
+    }
+  }
+  __threadfence();
+  __syncthreads();
+}
 // Every transform block of one plane of block b (code_plane, k_recon.h:190-291).
 __device__ long long code_plane(const Ctx &c, Smem &sm, int plane, int txSz) {
   const FrameParams *fp = c.fp;
@@ -431,8 +487,8 @@ __device__ long long code_plane(const Ctx &c, Smem &sm, int plane, int txSz) {
         pred::IntraArgs a;
         a.haveLeft = AvailL || x > 0;
         a.haveAbove = AvailU || y > 0;
-        a.haveAboveRight = BD(sm, plane, (sbr >> sub) - 1, (sbc >> sub) + stepX);
-        a.haveBelowLeft = BD(sm, plane, (sbr >> sub) + stepY, (sbc >> sub) - 1);
+        a.haveAboveRight = decoded(c, sm, plane, (sbr >> sub) - 1, (sbc >> sub) + stepX, 1);
+        a.haveBelowLeft = decoded(c, sm, plane, (sbr >> sub) + stepY, (sbc >> sub) - 1, 0);
         int isCfl = plane > 0 && b.uv_mode == UV_CFL_PRED;
         a.mode = plane == 0 ? b.y_mode : (isCfl ? DC_PRED : b.uv_mode);
         a.angleDelta = plane == 0 ? b.angle_y : b.angle_uv;
@@ -444,6 +500,7 @@ __device__ long long code_plane(const Ctx &c, Smem &sm, int plane, int txSz) {
         a.filterType = (b.interp_filter >> (plane == 0 ? 4 : 5)) & 1;
         pred::IntraState st;
         pred::intra_state(a, &st);
+        wait_edges(c, sm, plane, a, startX, startY);
         pred::intra_edges(px, rs, startX, startY, a, st, above, left, etmp, (int)threadIdx.x, RT, CtaSync());
         int tw = 1 << a.log2W, th = 1 << a.log2H;
         int dcv = a.mode == DC_PRED ? pred::intra_dc(a, above, left) : 0;
@@ -489,13 +546,9 @@ __device__ long long code_plane(const Ctx &c, Smem &sm, int plane, int txSz) {
       int eob = code_tx(c, sm, spx, stride, px, rs, startX, startY, txSz, plane, cands, numCands,
                         c.coefs + b.coef_off[plane] + txIdx * T(Tx_Width)[txSz] * T(Tx_Height)[txSz], &t, &cst);
       total += cst;
-      if (threadIdx.x == 0) {
-        if (plane == 0) {
-          tx_type_set(b, txIdx, t);
-          if (txIdx == 0) b.tx_type = t;
-        }
-        for (int i = 0; i < stepY; i++)
-          for (int j = 0; j < stepX; j++) BD(sm, plane, (sbr >> sub) + i, (sbc >> sub) + j) = 1;
+      if (threadIdx.x == 0 && plane == 0) {
+        tx_type_set(b, txIdx, t);
+        if (txIdx == 0) b.tx_type = t;
       }
       txIdx++;
       anyNz |= eob > 0;
@@ -505,27 +558,6 @@ __device__ long long code_plane(const Ctx &c, Smem &sm, int plane, int txSz) {
   if (threadIdx.x == 0) b.eob[plane] = anyNz;
   __syncthreads();
   return total;
-}
-
-// The BlockDecoded marks code_plane leaves for an inter block (phase 1).
-__device__ void mark_bd_inter(const FrameParams *fp, Smem &sm, const BlockInfo &b) {
-  if (threadIdx.x != 0) return;
-  for (int plane = 0; plane < 3; plane++) {
-    int sub = plane > 0;
-    int txSz = fp->lossless ? TX_4X4 : plane > 0 ? uv_tx_size(b.bsize, 1, 1) : T(Max_Tx_Size_Rect)[b.bsize];
-    int planeSz = T(Subsampled_Size)[b.bsize][sub][sub];
-    int num4x4W = T(Num_4x4_Blocks_Wide)[planeSz], num4x4H = T(Num_4x4_Blocks_High)[planeSz];
-    int baseX = (b.mi_col >> sub) * 4, baseY = (b.mi_row >> sub) * 4;
-    int stepX = T(Tx_Width)[txSz] >> 2, stepY = T(Tx_Height)[txSz] >> 2;
-    for (int y = 0; y < num4x4H; y += stepY)
-      for (int x = 0; x < num4x4W; x += stepX) {
-        int startX = baseX + 4 * x, startY = baseY + 4 * y;
-        if (startX >= ((fp->mi_cols * 4) >> sub) || startY >= ((fp->mi_rows * 4) >> sub)) continue;
-        int sbr = ((startY << sub) >> 2) & 15, sbc = ((startX << sub) >> 2) & 15;
-        for (int i = 0; i < stepY; i++)
-          for (int j = 0; j < stepX; j++) BD(sm, plane, (sbr >> sub) + i, (sbc >> sub) + j) = 1;
-      }
-  }
 }
 
 // One block (recon_block, k_recon.h:293-394); sm.blk holds it.
@@ -611,13 +643,13 @@ __device__ void recon_block(const Ctx &c, Smem &sm, BlockInfo *gb) {
       code_plane(c, sm, 0, T(Max_Tx_Size_Rect)[bs]);
       continue;
     }
-    // tx_depth RD search: every depth from the same pixels and BlockDecoded
-    // flags, the winner re-coded last unless it already was
+    // tx_depth RD search: every depth from the same pixels (BlockDecoded
+    // inside the block follows the depth's own transform order), the winner
+    // re-coded last unless it already was
     int w = block_w(bs), h = block_h(bs);
     int rs = sm.rstride[0];
     uint8_t *px = sm.recp[0] + baseY * rs + baseX;
     for (int k = tid; k < w * h; k += RT) sm.save[k] = px[(k / w) * rs + (k % w)];
-    for (int k = tid; k < BD_DIM * BD_DIM; k += RT) sm.bdsave[k] = sm.bd[k];
     __syncthreads();
     long long best = -1;
     int bestD = 0;
@@ -626,7 +658,6 @@ __device__ void recon_block(const Ctx &c, Smem &sm, BlockInfo *gb) {
       if (d == maxDepth + 1 && bestD == maxDepth) break;
       if (d > 0) {
         for (int k = tid; k < w * h; k += RT) px[(k / w) * rs + (k % w)] = sm.save[k];
-        for (int k = tid; k < BD_DIM * BD_DIM; k += RT) sm.bd[k] = sm.bdsave[k];
         __syncthreads();
       }
       long long cst = code_plane(c, sm, 0, depth_tx_size(bs, depth)) + (long long)fp->lambda * 8 * depth;
@@ -642,213 +673,89 @@ __device__ void recon_block(const Ctx &c, Smem &sm, BlockInfo *gb) {
   if (tid == 0) *gb = b;
 }
 
-// clear_block_decoded_flags( r, c, 16 ) (k_recon.h:402-414).
-__device__ void clear_bd(const FrameParams *fp, Smem &sm, int r, int c) {
-  for (int k = threadIdx.x; k < 3 * BD_DIM * BD_DIM; k += RT) sm.bd[k] = 0;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    for (int plane = 0; plane < 3; plane++) {
-      int sub = plane > 0;
-      int sbWidth4 = (tile_col_end(fp, c) - c) >> sub;
-      int sbHeight4 = (fp->mi_rows - r) >> sub;
-      for (int y = -1; y <= (16 >> sub); y++)
-        for (int x = -1; x <= (16 >> sub); x++) {
-          if (y < 0 && x < sbWidth4) BD(sm, plane, y, x) = 1;
-          else if (x < 0 && y < sbHeight4) BD(sm, plane, y, x) = 1;
-          else BD(sm, plane, y, x) = 0;
-        }
-      BD(sm, plane, 16 >> sub, -1) = 0;
-    }
+// Per frame, before the recon launch: the block index of every 4x4 luma
+// unit of the frame (one warp per superblock, lanes over a block's units).
+__global__ void k_block_map(const FrameParams *fp, const BlockInfo *blocks, const SbInfo *sbs, int *blkAt) {
+  int sb = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+  if (sb >= fp->sb_cols * fp->sb_rows) return;
+  SbInfo sbi = sbs[sb];
+  int cols = fp->mi_cols, rows = fp->mi_rows;
+  for (int k = 0; k < imin(sbi.num_blocks, MAX_BLOCKS_PER_SB); k++) {
+    int idx = sb * MAX_BLOCKS_PER_SB + k;
+    const BlockInfo &b = blocks[idx];
+    if (b.mi_row < 0 || b.mi_col < 0) continue;
+    int h = imax(0, imin(T(Num_4x4_Blocks_High)[b.bsize], rows - b.mi_row));
+    int w = imax(0, imin(T(Num_4x4_Blocks_Wide)[b.bsize], cols - b.mi_col));
+    for (int i = lane; i < w * h; i += 32) blkAt[(b.mi_row + i / w) * cols + b.mi_col + i % w] = idx;
   }
-  __syncthreads();
 }
 
-// Stages the superblock's reconstruction (final inter samples, the
-// neighbours' samples) into the shared tile and points the views at it; the
-// tile covers every sample intra prediction of the superblock can read (the
-// row above, extended over the above-right superblock, and the column to the
-// left). Loads go through L2: other CTAs of the launch wrote those samples.
-__device__ void tile_load(const Ctx &c, Smem &sm, int sbRow, int sbCol) {
-  const FrameParams *fp = c.fp;
-  for (int p = 0; p < 3; p++) {
-    int sub = p > 0, tw = sub ? TILE_C_W : TILE_Y_W, th = sub ? TILE_C_H : TILE_Y_H;
-    uint8_t *t = sm.tile + (p == 0 ? 0 : TILE_Y_BYTES + (p - 1) * TILE_C_BYTES);
-    int x0 = ((sbCol * 64) >> sub) - 1, y0 = ((sbRow * 64) >> sub) - 1;
-    int stride = fp->stride[p], ph = fp->plane_h[p];
-    const uint8_t *g = c.rec + fp->offset[p];
-    for (int k = threadIdx.x; k < tw * th; k += RT) {
-      int y = y0 + k / tw, x = x0 + k % tw;
-      t[k] = (x >= 0 && y >= 0 && x < stride && y < ph) ? (uint8_t)ldpx(g + (size_t)y * stride + x) : 0;
-    }
-    if (threadIdx.x == 0) {
-      // plane origin in tile coordinates: sample (x, y) at t[(y - y0) * tw + (x - x0)]
-      sm.recp[p] = t - ((ptrdiff_t)y0 * tw + x0);
-      sm.rstride[p] = tw;
-    }
-  }
+// The claim list: every block index, superblocks in wave order and decode
+// order inside each (a prefix sum of the superblocks' block counts over one
+// CTA), and its length.
+__global__ void __launch_bounds__(1024) k_block_order(const SbInfo *sbs, const int *order, int nsb, int *list,
+                                                      int *total) {
+  __shared__ int part[1024];
+  int t = threadIdx.x, per = (nsb + 1023) / 1024, s0 = imin(nsb, t * per), s1 = imin(nsb, s0 + per);
+  int sum = 0;
+  for (int i = s0; i < s1; i++) sum += imax(0, imin(sbs[order[i]].num_blocks, MAX_BLOCKS_PER_SB));
+  part[t] = sum;
   __syncthreads();
+  for (int off = 1; off < 1024; off <<= 1) {
+    int v = t >= off ? part[t - off] : 0;
+    __syncthreads();
+    part[t] += v;
+    __syncthreads();
+  }
+  int base = part[t] - sum;
+  for (int i = s0; i < s1; i++) {
+    int sb = order[i], n = imax(0, imin(sbs[sb].num_blocks, MAX_BLOCKS_PER_SB));
+    for (int k = 0; k < n; k++) list[base++] = sb * MAX_BLOCKS_PER_SB + k;
+  }
+  if (t == 1023) *total = part[1023];
 }
 
-// Writes the superblock's own samples from the tile back to the frame.
-__device__ void tile_store(const Ctx &c, Smem &sm, int sbRow, int sbCol) {
-  const FrameParams *fp = c.fp;
-  for (int p = 0; p < 3; p++) {
-    int sub = p > 0, n = 64 >> sub, tw = sub ? TILE_C_W : TILE_Y_W;
-    const uint8_t *t = sm.tile + (p == 0 ? 0 : TILE_Y_BYTES + (p - 1) * TILE_C_BYTES);
-    int x0 = (sbCol * 64) >> sub, y0 = (sbRow * 64) >> sub, stride = fp->stride[p];
-    uint8_t *g = c.rec + fp->offset[p];
-    for (int k = threadIdx.x; k < n * n; k += RT) {
-      int y = k / n, x = k % n;
-      g[(size_t)(y0 + y) * stride + x0 + x] = t[(y + 1) * tw + x + 1];
-    }
-  }
-  __syncthreads();
-}
+// Claim state of the recon launch: the list, its length and the counter.
+struct Claim {
+  const int *list;
+  const int *total;
+  int *next;
+};
 
-// Superblock sb, phase 0: its inter blocks; phase 1: its intra blocks in
-// decode order with BlockDecoded tracking (inter blocks only mark theirs).
-__device__ void recon_superblock(const Ctx &c, Smem &sm, int sb, int phase) {
+// Every block of the frame, one persistent launch: each CTA (one warp)
+// claims the next block of the list, codes it (waiting inside on the blocks
+// its intra edges read) and publishes its completion flag.
+__global__ void __launch_bounds__(RT, 1) k_recon_blocks(Ctx c, Claim q) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Smem &sm = *(Smem *)smem_raw;
   const FrameParams *fp = c.fp;
-  SbInfo sbi = c.sbs[sb];
-  if (phase == 0 && threadIdx.x < 3) {
+  if (threadIdx.x < 3) {
     int p = threadIdx.x;
     sm.recp[p] = c.rec + fp->offset[p];
     sm.rstride[p] = fp->stride[p];
   }
-  if (phase == 1) {
-    if (threadIdx.x == 0) {
-      int any = 0;
-      for (int k = 0; k < sbi.num_blocks; k++) any |= !c.blocks[sbi.first_block + k].is_inter;
-      sm.flag = any;
-    }
-    __syncthreads();
-    int any = sm.flag;
-    __syncthreads();
-    if (!any) return;
-    clear_bd(fp, sm, sbi.sb_row * 16, sbi.sb_col * 16);
-    tile_load(c, sm, sbi.sb_row, sbi.sb_col);
-  }
-  for (int k = 0; k < sbi.num_blocks; k++) {
-    BlockInfo *gb = &c.blocks[sbi.first_block + k];
-    if (threadIdx.x == 0) sm.blk = *gb;
-    __syncthreads();
-    int inter = sm.blk.is_inter;
-    if (phase == 0 ? inter : !inter) {
-      recon_block(c, sm, gb);
-    } else if (phase == 1) {
-      mark_bd_inter(fp, sm, sm.blk);
-    }
-    __syncthreads();
-  }
-  if (phase == 1) tile_store(c, sm, sbi.sb_row, sbi.sb_col);
-}
-
-// Phase 0 over every superblock (one CTA each): the frame's inter blocks.
-__global__ void __launch_bounds__(RT) k_recon_inter(Ctx c) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  Smem &sm = *(Smem *)smem_raw;
-  recon_superblock(c, sm, blockIdx.x, 0);
-}
-
-// Dependency state of the intra phase: a claim counter over the superblock
-// order (waves, see the file comment), one completion flag per superblock,
-// and the status word (0 ok; 1 a dependency wait gave up) with an abort flag.
-struct IntraSync {
-  const int *order;  // superblocks in wave order
-  int n;
-  int *next;         // claim counter
-  int *done;         // per superblock: 1 once its intra blocks are written
-  int *status;       // [0] error code, [1] abort
-  const int *edges;  // per superblock: which of its edges an intra block touches
-};
-
-// Edge bits of a superblock's intra blocks: EDGE_L / EDGE_T mark intra blocks
-// that may read across its left / top boundary (they touch it); EDGE_R /
-// EDGE_B mark intra blocks whose samples lie along its right / bottom edge.
-enum { EDGE_L = 1, EDGE_T = 2, EDGE_R = 4, EDGE_B = 8 };
-
-// One warp per superblock.
-__global__ void k_intra_edges(const FrameParams *fp, const BlockInfo *blocks, const SbInfo *sbs, int *edges) {
-  int sb = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
-  if (sb >= fp->sb_cols * fp->sb_rows) return;
-  SbInfo sbi = sbs[sb];
-  int r0 = sbi.sb_row * 16, c0 = sbi.sb_col * 16, m = 0;
-  for (int k = lane; k < sbi.num_blocks; k += 32) {
-    const BlockInfo &b = blocks[sbi.first_block + k];
-    if (b.is_inter) continue;
-    int w4 = T(Num_4x4_Blocks_Wide)[b.bsize], h4 = T(Num_4x4_Blocks_High)[b.bsize];
-    if (b.mi_col == c0) m |= EDGE_L;
-    if (b.mi_row == r0) m |= EDGE_T;
-    if (b.mi_col + w4 >= c0 + 16) m |= EDGE_R;
-    if (b.mi_row + h4 >= r0 + 16) m |= EDGE_B;
-  }
-  for (int off = 16; off > 0; off >>= 1) m |= __shfl_xor_sync(0xffffffffu, m, off);
-  if (lane == 0) edges[sb] = m;
-}
-
-#define SPIN_LIMIT (1 << 22)  // x ~256 ns sleeps: about a second, far above any frame's recon
-
-// Phase 1 as one persistent launch: each CTA claims the next superblock in
-// wave order, waits until its left and above-right neighbours (same tile
-// column) have completed, codes its intra blocks and publishes completion.
-// Claims are in a topological order and a claimed superblock is always held
-// by a running CTA, so every wait ends; a wait that still exceeds the limit
-// sets the status and aborts the launch instead of hanging.
-__global__ void __launch_bounds__(RT) k_recon_intra(Ctx c, IntraSync q) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  Smem &sm = *(Smem *)smem_raw;
-  const FrameParams *fp = c.fp;
-  volatile int *vdone = q.done;
-  volatile int *vstatus = q.status;
+  volatile int *vstatus = c.status;
+  int total = *q.total;
   for (;;) {
     if (threadIdx.x == 0) {
-      int item = vstatus[1] ? q.n : atomicAdd(q.next, 1);
-      int ok = item < q.n;
-      if (ok) {
-        int sb = q.order[item];
-        int r = sb / fp->sb_cols, col = sb % fp->sb_cols;
-        int ts = (col / fp->tile_w_sb) * fp->tile_w_sb, te = imin(fp->sb_cols, ts + fp->tile_w_sb);
-        // the neighbours in the tile column whose intra samples this
-        // superblock's intra blocks can read: left (left column), above-left
-        // (corner sample), above and above-right (row above); a neighbour
-        // whose touching edge holds only inter samples (final since phase 0)
-        // imposes no wait. All four precede this superblock in wave order.
-        int me = q.edges[sb], deps[4], nd = 0;
-        if (col > ts && (me & EDGE_L) && (q.edges[sb - 1] & EDGE_R)) deps[nd++] = sb - 1;
-        if (r > 0 && (me & EDGE_T)) {
-          int up = sb - fp->sb_cols;
-          if (col > ts && (q.edges[up - 1] & EDGE_B)) deps[nd++] = up - 1;
-          if (q.edges[up] & EDGE_B) deps[nd++] = up;
-          if (col + 1 < te && (q.edges[up + 1] & EDGE_B)) deps[nd++] = up + 1;
-        }
-        for (int d = 0; d < nd && ok; d++) {
-          int spins = 0;
-          while (!vdone[deps[d]]) {
-            if (vstatus[1] || ++spins > SPIN_LIMIT) {
-              if (!vstatus[1]) {
-                atomicExch(q.status, 1);
-                atomicExch(q.status + 1, 1);
-              }
-              ok = 0;
-              break;
-            }
-            __nanosleep(256);
-          }
-        }
-        __threadfence();
-        sm.flag = ok ? sb : -1;
-      } else {
-        sm.flag = -1;
+      int item = vstatus[1] ? total : atomicAdd(q.next, 1);
+      int me = item < total ? q.list[item] : -1;
+      sm.flag = me;
+      if (me >= 0) {
+        int sb = me / MAX_BLOCKS_PER_SB;
+        sm.me = me;
+        sm.r0 = (sb / fp->sb_cols) * 16;
+        sm.c0 = (sb % fp->sb_cols) * 16;
+        sm.blk = c.blocks[me];
       }
     }
     __syncthreads();
-    int sb = sm.flag;
-    __syncthreads();
-    if (sb < 0) return;
-    recon_superblock(c, sm, sb, 1);
+    int me = sm.flag;
+    if (me < 0) return;
+    recon_block(c, sm, c.blocks + me);
     __threadfence();
     __syncthreads();
-    if (threadIdx.x == 0) atomicExch(q.done + sb, 1);
+    if (threadIdx.x == 0) atomicExch(c.done + me, 1);
   }
 }
 

@@ -64,11 +64,12 @@ struct mav1cu_session {
   uint8_t *qp[2];          // 16 quarter-pel planes per reference
   uint8_t *dsrc, *dref[2]; // decimated planes
   uint8_t *ys, *uvs;       // edge-type marks per mi
-  int *waves;              // superblock lists of the intra waves
-  int *status;             // device status: [0] error, [1] abort, [2] claim counter
-  int *sb_done;            // per-superblock completion flags of the intra phase
-  int *sb_edges;           // per-superblock edge bits of its intra blocks
-  int resident_recon;      // CTAs of the intra phase (co-resident)
+  int *waves;              // superblocks in wave order
+  int *status;             // device status: [0] error, [1] abort, [2] claim counter, [3] claim list length
+  int *blk_at;             // block index per 4x4 luma unit
+  int *blk_list;           // recon claim list
+  int *blk_done;           // per-block completion flags of the recon launch
+  int resident_recon;      // recon workers (one-warp CTAs) resident at once
   std::vector<int> wave_start, wave_len;
   int wave_tile_w;
   FrameParams fp;          // host copy of the current parameters
@@ -226,7 +227,8 @@ extern "C" void mav1cu_build_fwd_matrices(int32_t *mats) {
 static void free_all(mav1cu_session *s) {
   for (int i = 0; i < MAV1CU_BUF_COUNT; i++)
     if (s->buf[i]) cudaFree(s->buf[i]);
-  void *extra[] = {s->qp[0], s->qp[1], s->dsrc, s->dref[0], s->dref[1], s->ys, s->uvs, s->waves, s->status, s->sb_done, s->sb_edges};
+  void *extra[] = {s->qp[0], s->qp[1], s->dsrc, s->dref[0], s->dref[1], s->ys, s->uvs, s->waves, s->status, s->blk_at, s->blk_list,
+                   s->blk_done};
   for (void *p : extra)
     if (p) cudaFree(p);
   if (s->own_stream) cudaStreamDestroy(s->own_stream);
@@ -273,8 +275,9 @@ extern "C" int mav1cu_session_create(int width, int height, int max_cdef_presets
   if (e == cudaSuccess) e = cudaMalloc(&s->uvs, (size_t)g.mi_rows * g.mi_cols);
   if (e == cudaSuccess) e = cudaMalloc(&s->waves, sizeof(int) * nsb);
   if (e == cudaSuccess) e = cudaMalloc(&s->status, sizeof(int) * 4);
-  if (e == cudaSuccess) e = cudaMalloc(&s->sb_done, sizeof(int) * nsb);
-  if (e == cudaSuccess) e = cudaMalloc(&s->sb_edges, sizeof(int) * nsb);
+  if (e == cudaSuccess) e = cudaMalloc(&s->blk_at, sizeof(int) * g.mi_rows * g.mi_cols);
+  if (e == cudaSuccess) e = cudaMalloc(&s->blk_list, sizeof(int) * MAX_BLOCKS_PER_SB * nsb);
+  if (e == cudaSuccess) e = cudaMalloc(&s->blk_done, sizeof(int) * MAX_BLOCKS_PER_SB * nsb);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->own_stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) {
     snprintf(err, errlen, "device allocation failed: %s", cudaGetErrorString(e));
@@ -284,6 +287,7 @@ extern "C" int mav1cu_session_create(int width, int height, int max_cdef_presets
   }
   s->stream = s->own_stream;
   cudaMemset(s->status, 0, sizeof(int) * 4);
+  cudaMemset(s->blk_at, 0xff, sizeof(int) * g.mi_rows * g.mi_cols);  // -1: no block
   std::vector<int32_t> mats(4096 * 15);
   mav1cu_build_fwd_matrices(mats.data());
   cudaMemcpy(s->buf[MAV1CU_BUF_MATS], mats.data(), mats.size() * sizeof(int32_t), cudaMemcpyHostToDevice);
@@ -293,13 +297,12 @@ extern "C" int mav1cu_session_create(int width, int height, int max_cdef_presets
     mav1cu_session_destroy(s);
     return code;
   }
-  cudaFuncSetAttribute(rec::k_recon_inter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(rec::Smem));
-  cudaFuncSetAttribute(rec::k_recon_intra, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(rec::Smem));
+  cudaFuncSetAttribute(rec::k_recon_blocks, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(rec::Smem));
   {
     int dev = 0, sms = 0, per = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, rec::k_recon_intra, RT, sizeof(rec::Smem));
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, rec::k_recon_blocks, RT, sizeof(rec::Smem));
     s->resident_recon = imax(1, sms * imax(1, per));
   }
   cudaFuncSetAttribute(ana::k_analyze_level, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -350,8 +353,9 @@ extern "C" int mav1cu_copy(mav1cu_session *s, int dst, int src, size_t bytes) {
   return check_cuda(s, cudaMemcpyAsync(s->buf[dst], s->buf[src], bytes, cudaMemcpyDeviceToDevice, s->stream), "copy");
 }
 
-// Superblock lists of the intra waves: wave (c - tileStart) + 2r holds the
-// superblocks whose left and above-right neighbours are in earlier waves.
+// Superblocks in wave order: wave (c - tileStart) + 2r holds the superblocks
+// whose left, above-left, above and above-right neighbours (same tile
+// column) are in earlier waves. The recon claim list follows this order.
 static int build_waves(mav1cu_session *s, int tile_w_sb) {
   const Geometry &g = s->g;
   int nw = tile_w_sb + 2 * (g.sb_rows - 1);
@@ -483,28 +487,27 @@ extern "C" int mav1cu_recon(mav1cu_session *s) {
   c.coefs = (int32_t *)s->buf[MAV1CU_BUF_COEFS];
   c.mats = (const int32_t *)s->buf[MAV1CU_BUF_MATS];
   c.status = s->status;
-  size_t smem = sizeof(rec::Smem);
-  if (!s->fp.frame_is_intra) {
-    rec::k_recon_inter<<<s->g.num_sbs, RT, smem, s->stream>>>(c);
-    if (after_launch(s, "recon inter blocks")) return s->err;
+  c.blk_at = s->blk_at;
+  c.done = s->blk_done;
+  int nsb = s->g.num_sbs;
+  // leaf frames hold inter blocks only (the analysis never keeps intra
+  // there): no intra edge reads, no unit map
+  if (!(s->fp.leaf && !s->fp.frame_is_intra)) {
+    rec::k_block_map<<<(nsb + 3) / 4, 128, 0, s->stream>>>(DP(s), c.blocks, c.sbs, s->blk_at);
+    if (after_launch(s, "recon unit map")) return s->err;
   }
-  // leaf frames code inter blocks only (the analysis never keeps intra there)
-  if (s->fp.leaf && !s->fp.frame_is_intra) return MAV1CU_OK;
-  rec::IntraSync q;
-  q.order = s->waves;
-  q.n = s->g.num_sbs;
-  q.next = s->status + 2;
-  q.done = s->sb_done;
-  q.status = s->status;
-  q.edges = s->sb_edges;
-  rec::k_intra_edges<<<(s->g.num_sbs + 3) / 4, 128, 0, s->stream>>>(DP(s), c.blocks, c.sbs, s->sb_edges);
-  if (after_launch(s, "intra edges")) return s->err;
-  if (check_cuda(s, cudaMemsetAsync(s->sb_done, 0, sizeof(int) * s->g.num_sbs, s->stream), "recon flags") ||
+  rec::k_block_order<<<1, 1024, 0, s->stream>>>(c.sbs, s->waves, nsb, s->blk_list, s->status + 3);
+  if (after_launch(s, "recon claim list")) return s->err;
+  if (check_cuda(s, cudaMemsetAsync(s->blk_done, 0, sizeof(int) * MAX_BLOCKS_PER_SB * nsb, s->stream),
+                 "recon flags") ||
       check_cuda(s, cudaMemsetAsync(s->status + 2, 0, sizeof(int), s->stream), "recon counter"))
     return s->err;
-  int grid = imin(s->g.num_sbs, s->resident_recon);
-  rec::k_recon_intra<<<grid, RT, smem, s->stream>>>(c, q);
-  return after_launch(s, "recon intra blocks");
+  rec::Claim q;
+  q.list = s->blk_list;
+  q.total = s->status + 3;
+  q.next = s->status + 2;
+  rec::k_recon_blocks<<<s->resident_recon, RT, sizeof(rec::Smem), s->stream>>>(c, q);
+  return after_launch(s, "recon");
 }
 
 extern "C" int mav1cu_frame_core(mav1cu_session *s) {
@@ -570,7 +573,7 @@ extern "C" int mav1cu_synchronize(mav1cu_session *s) {
   if (check_cuda(s, cudaStreamSynchronize(s->stream), "synchronize")) return s->err;
   int st[2] = {0, 0};
   if (check_cuda(s, cudaMemcpy(st, s->status, sizeof st, cudaMemcpyDeviceToHost), "status")) return s->err;
-  if (st[0]) return set_error(s, MAV1CU_ERR_DEVICE, "device status %d: an intra-phase dependency wait gave up", st[0]);
+  if (st[0]) return set_error(s, MAV1CU_ERR_DEVICE, "device status %d: a recon dependency wait gave up", st[0]);
   return MAV1CU_OK;
 }
 
