@@ -150,32 +150,24 @@ HD void intra_state(const IntraArgs &a, IntraState *s) {
 }
 
 // Edge sample i (0 <= i < w + h) of AboveRow / LeftCol before filtering.
-// L2 selects reads through L2 (ldpx) for a frame other CTAs write during the
-// launch; plain loads otherwise (the analysis reads the source).
-template <bool L2 = false>
-HD int edge_px(const uint8_t *p) { return L2 ? ldpx(p) : *p; }
-
-template <bool L2 = false>
 HD int above_sample(const uint8_t *px, int stride, int x, int y, const IntraArgs &a, int i) {
   int w = 1 << a.log2W;
-  if (!a.haveAbove && a.haveLeft) return edge_px<L2>(px + y * stride + x - 1);
+  if (!a.haveAbove && a.haveLeft) return px[y * stride + x - 1];
   if (!a.haveAbove && !a.haveLeft) return (1 << 7) - 1;
   int aboveLimit = imin(a.maxX, x + (a.haveAboveRight ? 2 * w : w) - 1);
-  return edge_px<L2>(px + (y - 1) * stride + imin(aboveLimit, x + i));
+  return px[(y - 1) * stride + imin(aboveLimit, x + i)];
 }
-template <bool L2 = false>
 HD int left_sample(const uint8_t *px, int stride, int x, int y, const IntraArgs &a, int i) {
   int h = 1 << a.log2H;
-  if (!a.haveLeft && a.haveAbove) return edge_px<L2>(px + (y - 1) * stride + x);
+  if (!a.haveLeft && a.haveAbove) return px[(y - 1) * stride + x];
   if (!a.haveLeft && !a.haveAbove) return (1 << 7) + 1;
   int leftLimit = imin(a.maxY, y + (a.haveBelowLeft ? 2 * h : h) - 1);
-  return edge_px<L2>(px + imin(leftLimit, y + i) * stride + x - 1);
+  return px[imin(leftLimit, y + i) * stride + x - 1];
 }
-template <bool L2 = false>
 HD int corner_sample(const uint8_t *px, int stride, int x, int y, const IntraArgs &a) {
-  if (a.haveAbove && a.haveLeft) return edge_px<L2>(px + (y - 1) * stride + x - 1);
-  if (a.haveAbove) return edge_px<L2>(px + (y - 1) * stride + x);
-  if (a.haveLeft) return edge_px<L2>(px + y * stride + x - 1);
+  if (a.haveAbove && a.haveLeft) return px[(y - 1) * stride + x - 1];
+  if (a.haveAbove) return px[(y - 1) * stride + x];
+  if (a.haveLeft) return px[y * stride + x - 1];
   return 1 << 7;
 }
 
@@ -188,10 +180,10 @@ __host__ __device__ void intra_edges(const uint8_t *px, int stride, int x, int y
                             int *above, int *left, int *tmp, int rank, int n, Sync sync) {
   int w = 1 << a.log2W, h = 1 << a.log2H;
   for (int i = rank; i < w + h; i += n) {
-    above[i] = above_sample<true>(px, stride, x, y, a, i);
-    left[i] = left_sample<true>(px, stride, x, y, a, i);
+    above[i] = above_sample(px, stride, x, y, a, i);
+    left[i] = left_sample(px, stride, x, y, a, i);
   }
-  if (rank == 0) above[-1] = left[-1] = corner_sample<true>(px, stride, x, y, a);
+  if (rank == 0) above[-1] = left[-1] = corner_sample(px, stride, x, y, a);
   sync();
   if (!intra_is_directional(a.mode) || !a.edgeFilter) return;
   int pAngle = s.pAngle;

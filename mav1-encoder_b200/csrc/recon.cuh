@@ -63,6 +63,10 @@ struct Ctx {
   int *done;            // per block index: 1 once its samples are written
 };
 
+#define TILE_Y 129     // 2 * 64 + 1
+#define TILE_C 65      // 2 * 32 + 1
+#define FMAT_SMALL 336 // 4 * 4 + 8 * 8 + 16 * 16
+
 struct Smem {
   int32_t resid[64 * 64];  // residual, then the inverse transform's plane
   int32_t tmp[64 * 32];    // forward row pass output
@@ -76,9 +80,22 @@ struct Smem {
   int flag;
   int me;      // index of the block being coded
   int r0, c0;  // its superblock's first 4x4 row / column
-  // the reconstruction: plane origins (absolute plane coordinates), strides
+  // views of the reconstruction and the source: plane origins (absolute
+  // plane coordinates) and strides; the frames for an inter block, the
+  // tiles below for an intra block
   uint8_t *recp[3];
   int rstride[3];
+  const uint8_t *srcp[3];
+  int sstride[3];
+  int sbBlk[256];            // block index of each 4x4 luma unit of the superblock (-1: outside the frame)
+  int32_t fmat[3][FMAT_SMALL];  // forward matrices of lengths 4, 8, 16 per kind
+  // intra block tiles: rows and columns -1 .. 2n - 1 around the block (its
+  // own samples, the above row over the above-right units, the left column
+  // over the below-left units), and its source
+  uint8_t tileY[TILE_Y * TILE_Y];
+  uint8_t tileC[2][TILE_C * TILE_C];
+  uint8_t srcY[64 * 64];
+  uint8_t srcC[2][32 * 32];
 };
 
 // Sums / maxima over the worker (one warp); the __syncwarp()s order the
@@ -101,6 +118,55 @@ struct CtaSync {
   __device__ void operator()() const { __syncthreads(); }
 };
 
+// One row of the inverse transform at a fixed width: dequantised levels ->
+// row transform -> clamp, into sm.resid (stride 64).
+template <int LW>
+__device__ void inv_row(Smem &sm, const int32_t *q, int i, int th, int dcQ, int acQ, int denom, int rect, int rk,
+                        int rowShift) {
+  constexpr int W = 1 << LW, TW = W < 32 ? W : 32;
+  int32_t t[W];
+  int nz = 0;
+#pragma unroll
+  for (int j = 0; j < W; j++) {
+    t[j] = (j < TW && i < th) ? tx::dequant_level(q[i * TW + j], (i == 0 && j == 0) ? dcQ : acQ, denom) : 0;
+    nz |= t[j];
+  }
+  if (!nz) {
+#pragma unroll
+    for (int j = 0; j < W; j++) sm.resid[i * 64 + j] = 0;
+    return;
+  }
+  if (rect) {
+#pragma unroll
+    for (int j = 0; j < W; j++) t[j] = (int32_t)round2l((int64_t)t[j] * 2896, 12);
+  }
+  tx::inverse_1d_n<LW>(t, rk, 16);
+#pragma unroll
+  for (int j = 0; j < W; j++) sm.resid[i * 64 + j] = clip3(-(1 << 15), (1 << 15) - 1, round2(t[j], rowShift));
+}
+
+// One column at a fixed height: column transform, then either added into the
+// reconstruction (flipped for FLIPADST types) or stored back into sm.resid.
+template <int LH>
+__device__ void inv_col(Smem &sm, int j, int w, int ck, int fud, int flr, uint8_t *rec, int rs, int x, int y) {
+  constexpr int H = 1 << LH;
+  int32_t t[H];
+#pragma unroll
+  for (int i = 0; i < H; i++) t[i] = sm.resid[i * 64 + j];
+  tx::inverse_1d_n<LH>(t, ck, 16);
+  if (rec) {
+    uint8_t *col = rec + y * rs + x + (flr ? (w - 1 - j) : j);
+#pragma unroll
+    for (int i = 0; i < H; i++) {
+      uint8_t *o = col + (fud ? (H - 1 - i) : i) * rs;
+      *o = (uint8_t)clip1((int)*o + round2(t[i], 4));
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < H; i++) sm.resid[i * 64 + j] = round2(t[i], 4);
+  }
+}
+
 // Levels of a candidate -> reconstruction residual (spec 7.13.3 with the
 // dequantisation of 7.12.3), into sm.resid (stride 64).
 // With rec set, the column pass adds its output straight into the
@@ -108,43 +174,37 @@ struct CtaSync {
 __device__ void inverse_2d(Smem &sm, const int32_t *q, int txSz, int txType, int dcQ, int acQ, uint8_t *rec = nullptr,
                            int rs = 0, int x = 0, int y = 0) {
   int lw = T(Tx_Width_Log2)[txSz], lh = T(Tx_Height_Log2)[txSz];
-  int w = 1 << lw, h = 1 << lh, tw = imin(32, w), th = imin(32, h);
+  int w = 1 << lw, h = 1 << lh, th = imin(32, h);
   int rowShift = T(Transform_Row_Shift)[txSz], denom = tx::dq_denom(txSz);
   int rect = iabs(lw - lh) == 1;
   int rk = tx::row_kind(txType), ck = tx::col_kind(txType);
   for (int i = threadIdx.x; i < h; i += RT) {
-    int32_t t[64];
-    int nz = 0;
-    for (int j = 0; j < w; j++) {
-      t[j] = (i < th && j < tw) ? tx::dequant_level(q[i * tw + j], (i == 0 && j == 0) ? dcQ : acQ, denom) : 0;
-      nz |= t[j];
+    switch (lw) {
+      case 2: inv_row<2>(sm, q, i, th, dcQ, acQ, denom, rect, rk, rowShift); break;
+      case 3: inv_row<3>(sm, q, i, th, dcQ, acQ, denom, rect, rk, rowShift); break;
+      case 4: inv_row<4>(sm, q, i, th, dcQ, acQ, denom, rect, rk, rowShift); break;
+      case 5: inv_row<5>(sm, q, i, th, dcQ, acQ, denom, rect, rk, rowShift); break;
+      default: inv_row<6>(sm, q, i, th, dcQ, acQ, denom, rect, rk, rowShift); break;
     }
-    if (!nz) {
-      for (int j = 0; j < w; j++) sm.resid[i * 64 + j] = 0;
-      continue;
-    }
-    if (rect)
-      for (int j = 0; j < w; j++) t[j] = (int32_t)round2l((int64_t)t[j] * 2896, 12);
-    tx::inverse_1d(t, rk, lw, 16);
-    for (int j = 0; j < w; j++) sm.resid[i * 64 + j] = clip3(-(1 << 15), (1 << 15) - 1, round2(t[j], rowShift));
   }
   __syncthreads();
   int fud = tx::flip_ud(txType), flr = tx::flip_lr(txType);
   for (int j = threadIdx.x; j < w; j += RT) {
-    int32_t t[64];
-    for (int i = 0; i < h; i++) t[i] = sm.resid[i * 64 + j];
-    tx::inverse_1d(t, ck, lh, 16);
-    if (rec) {
-      uint8_t *col = rec + y * rs + x + (flr ? (w - 1 - j) : j);
-      for (int i = 0; i < h; i++) {
-        uint8_t *o = col + (fud ? (h - 1 - i) : i) * rs;
-        *o = (uint8_t)clip1((int)*o + round2(t[i], 4));
-      }
-    } else {
-      for (int i = 0; i < h; i++) sm.resid[i * 64 + j] = round2(t[i], 4);
+    switch (lh) {
+      case 2: inv_col<2>(sm, j, w, ck, fud, flr, rec, rs, x, y); break;
+      case 3: inv_col<3>(sm, j, w, ck, fud, flr, rec, rs, x, y); break;
+      case 4: inv_col<4>(sm, j, w, ck, fud, flr, rec, rs, x, y); break;
+      case 5: inv_col<5>(sm, j, w, ck, fud, flr, rec, rs, x, y); break;
+      default: inv_col<6>(sm, j, w, ck, fud, flr, rec, rs, x, y); break;
     }
   }
   __syncthreads();
+}
+
+// Forward matrix of a kind and length: lengths 4..16 from the CTA's shared
+// copy, 32 and 64 from the table in global memory.
+__device__ __forceinline__ const int32_t *fwd_matrix(const Ctx &c, const Smem &sm, int kind, int lg) {
+  return lg <= 4 ? sm.fmat[kind] + (lg == 2 ? 0 : lg == 3 ? 16 : 80) : c.mats + fwd_slot(kind, lg);
 }
 
 // Transform, quantise and reconstruct one transform block whose prediction
@@ -236,7 +296,7 @@ __device__ int code_tx(const Ctx &c, Smem &sm, const uint8_t *src, int stride, u
       sm.resid[i * 64 + j] = (int)src[(y + yy) * stride + x + xx] - (int)rec[(y + yy) * rs + x + xx];
     }
     __syncthreads();
-    const int32_t *Mh = c.mats + fwd_slot(tx::row_kind(t), lw), *Mv = c.mats + fwd_slot(tx::col_kind(t), lh);
+    const int32_t *Mh = fwd_matrix(c, sm, tx::row_kind(t), lw), *Mv = fwd_matrix(c, sm, tx::col_kind(t), lh);
     for (int k = tid; k < h * tw; k += RT) {
       int i = k / tw, kk = k % tw;
       const int32_t *r = sm.resid + i * 64, *m = Mh + kk * w;
@@ -394,43 +454,33 @@ __device__ int decoded(const Ctx &c, const Smem &sm, int plane, int y, int x, in
     if (x < 0) return y < ((fp->mi_rows - sm.r0) >> sub);
     return 0;
   }
-  int r = sm.r0 + (y << sub), col = sm.c0 + (x << sub);
-  if (r >= fp->mi_rows || col >= fp->mi_cols) return 0;
-  int b = c.blk_at[r * fp->mi_cols + col];
+  if (sm.r0 + (y << sub) >= fp->mi_rows || sm.c0 + (x << sub) >= fp->mi_cols) return 0;
+  int b = sm.sbBlk[(y << sub) * 16 + (x << sub)];
   return b == sm.me ? own : (b >= 0 && b < sm.me);
 }
 
 #define SPIN_LIMIT (1 << 22)  // polls of at least one L2 round trip each: about a second
 
-// Waits until every other block whose samples intra_edges reads for this
-// transform block is complete: the above row from the corner (or x) to the
-// above limit, the left column from the corner (or y) to the left limit.
-// Each lane polls the completion flag of the block covering one 4x4 unit.
-// The blocks waited on precede this one in the claim order, so the wait
+// Block index covering 4x4 luma unit (r, col): the superblock's map in
+// shared memory, else the frame's map (neighbouring superblocks).
+__device__ __forceinline__ int block_at(const Ctx &c, const Smem &sm, int r, int col) {
+  int dr = r - sm.r0, dc = col - sm.c0;
+  if ((unsigned)dr < 16u && (unsigned)dc < 16u) return sm.sbBlk[dr * 16 + dc];
+  return c.blk_at[r * c.fp->mi_cols + col];
+}
+
+// Waits until the block covering each 4x4 unit of a run of n units
+// (first (r, col), step (dr, dc)) is complete, unless it is this block.
+// Every block waited on precedes this one in the claim order, so the wait
 // ends; past the limit it sets the error and abort words and gives up, and
 // every other wait then stops too.
-__device__ void wait_edges(const Ctx &c, Smem &sm, int plane, const pred::IntraArgs &a, int x, int y) {
-  const FrameParams *fp = c.fp;
-  int sub = plane > 0, w = 1 << a.log2W, h = 1 << a.log2H;
-  int nA = 0, nL = 0, rowA = 0, colA0 = 0, colL = 0, rowL0 = 0;
-  if (a.haveAbove) {
-    int lim = imin(imin(a.maxX, x + (a.haveAboveRight ? 2 * w : w) - 1), x + w + h - 1);
-    rowA = ((y - 1) << sub) >> 2;
-    colA0 = ((a.haveLeft ? x - 1 : x) << sub) >> 2;
-    nA = ((lim << sub) >> 2) - colA0 + 1;
-  }
-  if (a.haveLeft) {
-    int lim = imin(imin(a.maxY, y + (a.haveBelowLeft ? 2 * h : h) - 1), y + w + h - 1);
-    colL = ((x - 1) << sub) >> 2;
-    rowL0 = ((a.haveAbove ? y - 1 : y) << sub) >> 2;
-    nL = ((lim << sub) >> 2) - rowL0 + 1;
-  }
+__device__ void wait_units(const Ctx &c, const Smem &sm, int r, int col, int dr, int dc, int n) {
   volatile const int *vdone = c.done;
   volatile int *vstatus = c.status;
-  for (int i = threadIdx.x; i < nA + nL; i += RT) {
-    int r = i < nA ? rowA : rowL0 + (i - nA), col = i < nA ? colA0 + i : colL;
-    int b = c.blk_at[r * fp->mi_cols + col];
-    if (b == sm.me || (unsigned)b >= (unsigned)(fp->sb_cols * fp->sb_rows * MAX_BLOCKS_PER_SB)) continue;
+  int nblk = c.fp->sb_cols * c.fp->sb_rows * MAX_BLOCKS_PER_SB;
+  for (int i = threadIdx.x; i < n; i += RT) {
+    int b = block_at(c, sm, r + i * dr, col + i * dc);
+    if (b == sm.me || (unsigned)b >= (unsigned)nblk) continue;
     int spins = 0;
     while (!vdone[b]) {
       if (vstatus[1] || ++spins > SPIN_LIMIT) {
@@ -443,9 +493,101 @@ __device__ void wait_edges(const Ctx &c, Smem &sm, int plane, const pred::IntraA
       __nanosleep(64);
     }
   }
+}
+
+// Stages an intra block in shared memory: the superblock's unit map, the
+// block's own samples of every plane (the reconstruction so far, overwritten
+// as it is coded) and its source; then, once the blocks that wrote them are
+// complete, the edge samples its transform blocks can read. Those are the
+// row above and the column left of the block, extended past its corner by
+// the largest candidate transform's shorter side where the above-right /
+// below-left unit is decoded: the union of the samples intra_edges reads
+// (above / left limits, spec 7.11.2) over every transform block of every
+// candidate size. The views then point at the tiles.
+__device__ void stage_intra(const Ctx &c, Smem &sm) {
+  const FrameParams *fp = c.fp;
+  const BlockInfo &b = sm.blk;
+  int bs = b.bsize, tid = threadIdx.x;
+  for (int k = tid; k < 256; k += RT) {
+    int r = sm.r0 + (k >> 4), col = sm.c0 + (k & 15);
+    sm.sbBlk[k] = (r < fp->mi_rows && col < fp->mi_cols) ? c.blk_at[r * fp->mi_cols + col] : -1;
+  }
+  for (int p = 0; p < 3; p++) {
+    int sub = p > 0, S = sub ? TILE_C : TILE_Y;
+    uint8_t *t = sub ? sm.tileC[p - 1] : sm.tileY, *sb = sub ? sm.srcC[p - 1] : sm.srcY;
+    int lw = floor_log2(block_w(bs) >> sub), w = 1 << lw, h = block_h(bs) >> sub;
+    int x0 = (b.mi_col >> sub) * 4, y0 = (b.mi_row >> sub) * 4, fs = fp->stride[p];
+    const uint8_t *g = c.rec + fp->offset[p], *sp = c.src + fp->offset[p];
+    for (int k = tid; k < w * h; k += RT) {
+      int i = k >> lw, j = k & (w - 1);
+      t[(i + 1) * S + j + 1] = (uint8_t)ldpx(g + (y0 + i) * fs + x0 + j);
+      sb[k] = sp[(y0 + i) * fs + x0 + j];
+    }
+    if (tid == 0) {
+      sm.recp[p] = t + S + 1 - ((ptrdiff_t)y0 * S + x0);
+      sm.rstride[p] = S;
+      sm.srcp[p] = sb - ((ptrdiff_t)y0 * w + x0);
+      sm.sstride[p] = w;
+    }
+  }
+  __syncthreads();
+  int availU = b.mi_row > 0, availL = b.mi_col > tile_col_start(fp, b.mi_col);
+  int ay[3], ax0[3], ax1[3], ly0[3], ly1[3];
+  for (int p = 0; p < 3; p++) {
+    int sub = p > 0, w = block_w(bs) >> sub, h = block_h(bs) >> sub;
+    int x0 = (b.mi_col >> sub) * 4, y0 = (b.mi_row >> sub) * 4;
+    int txSz = fp->lossless ? TX_4X4 : sub ? uv_tx_size(bs, 1, 1) : T(Max_Tx_Size_Rect)[bs];
+    int ext = imin(T(Tx_Width)[txSz], T(Tx_Height)[txSz]);
+    int rowU = (b.mi_row & 15) >> sub, colU = (b.mi_col & 15) >> sub;
+    int ar = decoded(c, sm, p, rowU - 1, colU + (w >> 2), 0), bl = decoded(c, sm, p, rowU + (h >> 2), colU - 1, 0);
+    int maxX = ((fp->mi_cols * 4) >> sub) - 1, maxY = ((fp->mi_rows * 4) >> sub) - 1;
+    ay[p] = y0 - 1;
+    ax0[p] = x0 - availL;
+    ax1[p] = availU ? imin(maxX, x0 + w - 1 + (ar ? ext : 0)) : ax0[p] - 1;
+    ly0[p] = y0 - availU;
+    ly1[p] = availL ? imin(maxY, y0 + h - 1 + (bl ? ext : 0)) : ly0[p] - 1;
+    // the 4x4 luma units under those samples
+    if (ax1[p] >= ax0[p]) {
+      int c0 = (ax0[p] << sub) >> 2;
+      wait_units(c, sm, (ay[p] << sub) >> 2, c0, 0, 1, ((ax1[p] << sub) >> 2) - c0 + 1);
+    }
+    if (ly1[p] >= ly0[p]) {
+      int r0 = (ly0[p] << sub) >> 2;
+      wait_units(c, sm, r0, ((x0 - 1) << sub) >> 2, 1, 0, ((ly1[p] << sub) >> 2) - r0 + 1);
+    }
+  }
   __threadfence();
   __syncthreads();
+  for (int p = 0; p < 3; p++) {
+    int sub = p > 0, S = sub ? TILE_C : TILE_Y;
+    uint8_t *t = sub ? sm.tileC[p - 1] : sm.tileY;
+    int x0 = (b.mi_col >> sub) * 4, y0 = (b.mi_row >> sub) * 4, fs = fp->stride[p];
+    const uint8_t *g = c.rec + fp->offset[p];
+    for (int k = tid; k <= ax1[p] - ax0[p]; k += RT)
+      t[ax0[p] - x0 + 1 + k] = (uint8_t)ldpx(g + ay[p] * fs + ax0[p] + k);
+    for (int k = tid; k <= ly1[p] - ly0[p]; k += RT)
+      t[(ly0[p] - y0 + 1 + k) * S] = (uint8_t)ldpx(g + (ly0[p] + k) * fs + x0 - 1);
+  }
+  __syncthreads();
 }
+
+// Writes an intra block's own samples from its tiles to the frame.
+__device__ void unstage_intra(const Ctx &c, Smem &sm) {
+  const FrameParams *fp = c.fp;
+  const BlockInfo &b = sm.blk;
+  for (int p = 0; p < 3; p++) {
+    int sub = p > 0, S = sub ? TILE_C : TILE_Y;
+    const uint8_t *t = sub ? sm.tileC[p - 1] : sm.tileY;
+    int lw = floor_log2(block_w(b.bsize) >> sub), w = 1 << lw, h = block_h(b.bsize) >> sub;
+    int x0 = (b.mi_col >> sub) * 4, y0 = (b.mi_row >> sub) * 4, fs = fp->stride[p];
+    uint8_t *g = c.rec + fp->offset[p];
+    for (int k = threadIdx.x; k < w * h; k += RT) {
+      int i = k >> lw, j = k & (w - 1);
+      g[(y0 + i) * fs + x0 + j] = t[(i + 1) * S + j + 1];
+    }
+  }
+}
+
 // Every transform block of one plane of block b (code_plane, k_recon.h:190-291).
 __device__ long long code_plane(const Ctx &c, Smem &sm, int plane, int txSz) {
   const FrameParams *fp = c.fp;
@@ -456,10 +598,10 @@ __device__ long long code_plane(const Ctx &c, Smem &sm, int plane, int txSz) {
   int planeSz = T(Subsampled_Size)[bs][sub][sub];
   int num4x4W = T(Num_4x4_Blocks_Wide)[planeSz], num4x4H = T(Num_4x4_Blocks_High)[planeSz];
   int baseX = (MiCol >> sub) * 4, baseY = (MiRow >> sub) * 4;
-  int stride = fp->stride[plane];           // source
+  int stride = sm.sstride[plane];           // source view
+  const uint8_t *spx = sm.srcp[plane];
   uint8_t *px = sm.recp[plane];             // reconstruction view
   int rs = sm.rstride[plane];
-  const uint8_t *spx = c.src + fp->offset[plane];
   int stepX = T(Tx_Width)[txSz] >> 2, stepY = T(Tx_Height)[txSz] >> 2;
   int cands[16], numCands = 0;
   int isInter = b.is_inter;
@@ -500,7 +642,6 @@ __device__ long long code_plane(const Ctx &c, Smem &sm, int plane, int txSz) {
         a.filterType = (b.interp_filter >> (plane == 0 ? 4 : 5)) & 1;
         pred::IntraState st;
         pred::intra_state(a, &st);
-        wait_edges(c, sm, plane, a, startX, startY);
         pred::intra_edges(px, rs, startX, startY, a, st, above, left, etmp, (int)threadIdx.x, RT, CtaSync());
         int tw = 1 << a.log2W, th = 1 << a.log2H;
         int dcv = a.mode == DC_PRED ? pred::intra_dc(a, above, left) : 0;
@@ -574,7 +715,15 @@ __device__ void recon_block(const Ctx &c, Smem &sm, BlockInfo *gb) {
     b.tx_depth = 0;
     b.interp_filter &= 0x30;
   }
+  if (b.is_inter && threadIdx.x < 3) {
+    int p = threadIdx.x;
+    sm.recp[p] = c.rec + fp->offset[p];
+    sm.rstride[p] = fp->stride[p];
+    sm.srcp[p] = c.src + fp->offset[p];
+    sm.sstride[p] = fp->stride[p];
+  }
   __syncthreads();
+  if (!b.is_inter) stage_intra(c, sm);
   int tid = threadIdx.x;
   if (b.is_inter && fp->switchable_interp && !comp) {
     int w = block_w(bs), h = block_h(bs);
@@ -670,6 +819,7 @@ __device__ void recon_block(const Ctx &c, Smem &sm, BlockInfo *gb) {
     if (tid == 0) b.tx_depth = bestD;
     __syncthreads();
   }
+  if (!b.is_inter) unstage_intra(c, sm);
   if (tid == 0) *gb = b;
 }
 
@@ -729,11 +879,11 @@ __global__ void __launch_bounds__(RT, 1) k_recon_blocks(Ctx c, Claim q) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Smem &sm = *(Smem *)smem_raw;
   const FrameParams *fp = c.fp;
-  if (threadIdx.x < 3) {
-    int p = threadIdx.x;
-    sm.recp[p] = c.rec + fp->offset[p];
-    sm.rstride[p] = fp->stride[p];
-  }
+  for (int kind = 0; kind < 3; kind++)
+    for (int lg = 2; lg <= 4; lg++) {
+      int n = 1 << (2 * lg), off = lg == 2 ? 0 : lg == 3 ? 16 : 80;
+      for (int k = threadIdx.x; k < n; k += RT) sm.fmat[kind][off + k] = c.mats[fwd_slot(kind, lg) + k];
+    }
   volatile int *vstatus = c.status;
   int total = *q.total;
   for (;;) {

@@ -333,6 +333,21 @@ HD int flip_ud(int t) { return t == FLIPADST_DCT || t == FLIPADST_ADST || t == V
 HD int flip_lr(int t) { return t == DCT_FLIPADST || t == ADST_FLIPADST || t == H_FLIPADST || t == FLIPADST_FLIPADST; }
 
 // One 1-D inverse transform of kind / length 1 << log2n on t[0 .. n-1].
+// The same for a length fixed at compile time: every index of the working
+// array is a constant, so it stays in registers.
+template <int N>
+HD void inverse_1d_n(int32_t *t, int kind, int r) {
+  if (kind == KIND_DCT) {
+    idct<N>(t, r);
+  } else if (kind == KIND_ADST) {
+    if constexpr (N == 2) iadst4(t);
+    else if constexpr (N == 3) iadst8(t, r);
+    else if constexpr (N == 4) iadst16(t, r);
+  } else {
+    if constexpr (N <= 5) iidentity<N>(t);
+  }
+}
+
 HD void inverse_1d(int32_t *t, int kind, int log2n, int r) {
   if (kind == KIND_DCT) {
     switch (log2n) {
