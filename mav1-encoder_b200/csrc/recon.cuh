@@ -35,7 +35,10 @@
 
 namespace rec {
 
-#define RT 32  // threads per CTA: one warp, one block worker
+// Threads of the CTA coding a block: INTER_THREADS for the inter blocks of a
+// superblock, INTRA_THREADS (one warp) for an intra block worker.
+#define RT ((int)blockDim.x)
+constexpr int INTER_THREADS = 256, INTRA_THREADS = 32;
 #define FWD_SLOT_SIZE 4096
 HD int fwd_slot(int kind, int log2n) { return (kind * 5 + log2n - 2) * FWD_SLOT_SIZE; }
 
@@ -75,6 +78,7 @@ struct Smem {
   int edge[3][EDGE_LEN];   // AboveRow, LeftCol, filter copy
   uint8_t save[64 * 64];
   int sse33[33];
+  long long red[INTER_THREADS / 32];
   BlockInfo blk;
   int maxLumaW, maxLumaH;
   int flag;
@@ -98,21 +102,37 @@ struct Smem {
   uint8_t srcC[2][32 * 32];
 };
 
-// Sums / maxima over the worker (one warp); the __syncwarp()s order the
-// shared-memory writes before and after like a block barrier would.
-__device__ __forceinline__ long long cta_sum64(long long v, Smem &) {
-  __syncwarp();
+// Sums / maxima over the CTA. A one-warp CTA reduces by shuffles alone; the
+// __syncwarp()s order the shared-memory writes before and after like the
+// block barriers of the general path.
+__device__ __forceinline__ long long cta_sum64(long long v, Smem &sm) {
+  if (blockDim.x == 32) __syncwarp();
   for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
-  __syncwarp();
-  return v;
+  if (blockDim.x == 32) {
+    __syncwarp();
+    return v;
+  }
+  if ((threadIdx.x & 31) == 0) sm.red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  long long s = 0;
+  for (int k = 0; k < RT / 32; k++) s += sm.red[k];
+  __syncthreads();
+  return s;
 }
-__device__ __forceinline__ int cta_max(int v, Smem &) {
-  __syncwarp();
+__device__ __forceinline__ int cta_max(int v, Smem &sm) {
+  if (blockDim.x == 32) __syncwarp();
   for (int off = 16; off > 0; off >>= 1) v = imax(v, __shfl_xor_sync(0xffffffffu, v, off));
-  __syncwarp();
-  return v;
+  if (blockDim.x == 32) {
+    __syncwarp();
+    return v;
+  }
+  if ((threadIdx.x & 31) == 0) sm.red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  int m = 0;
+  for (int k = 0; k < RT / 32; k++) m = imax(m, (int)sm.red[k]);
+  __syncthreads();
+  return m;
 }
-static_assert(RT == 32, "the worker reductions assume one warp per CTA");
 
 struct CtaSync {
   __device__ void operator()() const { __syncthreads(); }
@@ -469,17 +489,22 @@ __device__ __forceinline__ int block_at(const Ctx &c, const Smem &sm, int r, int
   return c.blk_at[r * c.fp->mi_cols + col];
 }
 
-// Waits until the block covering each 4x4 unit of a run of n units
-// (first (r, col), step (dr, dc)) is complete, unless it is this block.
-// Every block waited on precedes this one in the claim order, so the wait
-// ends; past the limit it sets the error and abort words and gives up, and
-// every other wait then stops too.
-__device__ void wait_units(const Ctx &c, const Smem &sm, int r, int col, int dr, int dc, int n) {
+// Waits until the block covering each 4x4 unit of up to 6 runs of units
+// (run k: first (r[k], col[k]), along a row if row[k], else a column;
+// n[k] units) is complete, unless it is this block. Lanes take units of
+// all runs at once. Every block waited on precedes this one in the claim
+// order (or is an inter block, complete before the launch), so the wait
+// ends; past the limit it sets the error and abort words and gives up,
+// and every other wait then stops too.
+__device__ void wait_units(const Ctx &c, const Smem &sm, const int *r, const int *col, const int *row, const int *n) {
   volatile const int *vdone = c.done;
   volatile int *vstatus = c.status;
   int nblk = c.fp->sb_cols * c.fp->sb_rows * MAX_BLOCKS_PER_SB;
-  for (int i = threadIdx.x; i < n; i += RT) {
-    int b = block_at(c, sm, r + i * dr, col + i * dc);
+  int total = n[0] + n[1] + n[2] + n[3] + n[4] + n[5];
+  for (int i = threadIdx.x; i < total; i += RT) {
+    int k = 0, j = i;
+    while (j >= n[k]) j -= n[k++];
+    int b = block_at(c, sm, r[k] + (row[k] ? 0 : j), col[k] + (row[k] ? j : 0));
     if (b == sm.me || (unsigned)b >= (unsigned)nblk) continue;
     int spins = 0;
     while (!vdone[b]) {
@@ -533,6 +558,7 @@ __device__ void stage_intra(const Ctx &c, Smem &sm) {
   __syncthreads();
   int availU = b.mi_row > 0, availL = b.mi_col > tile_col_start(fp, b.mi_col);
   int ay[3], ax0[3], ax1[3], ly0[3], ly1[3];
+  int ur[6], uc[6], urow[6], un[6];  // the 4x4 luma units under the edge samples
   for (int p = 0; p < 3; p++) {
     int sub = p > 0, w = block_w(bs) >> sub, h = block_h(bs) >> sub;
     int x0 = (b.mi_col >> sub) * 4, y0 = (b.mi_row >> sub) * 4;
@@ -546,16 +572,16 @@ __device__ void stage_intra(const Ctx &c, Smem &sm) {
     ax1[p] = availU ? imin(maxX, x0 + w - 1 + (ar ? ext : 0)) : ax0[p] - 1;
     ly0[p] = y0 - availU;
     ly1[p] = availL ? imin(maxY, y0 + h - 1 + (bl ? ext : 0)) : ly0[p] - 1;
-    // the 4x4 luma units under those samples
-    if (ax1[p] >= ax0[p]) {
-      int c0 = (ax0[p] << sub) >> 2;
-      wait_units(c, sm, (ay[p] << sub) >> 2, c0, 0, 1, ((ax1[p] << sub) >> 2) - c0 + 1);
-    }
-    if (ly1[p] >= ly0[p]) {
-      int r0 = (ly0[p] << sub) >> 2;
-      wait_units(c, sm, r0, ((x0 - 1) << sub) >> 2, 1, 0, ((ly1[p] << sub) >> 2) - r0 + 1);
-    }
+    ur[2 * p] = (ay[p] << sub) >> 2;
+    uc[2 * p] = (ax0[p] << sub) >> 2;
+    urow[2 * p] = 1;
+    un[2 * p] = ax1[p] >= ax0[p] ? ((ax1[p] << sub) >> 2) - uc[2 * p] + 1 : 0;
+    ur[2 * p + 1] = (ly0[p] << sub) >> 2;
+    uc[2 * p + 1] = ((x0 - 1) << sub) >> 2;
+    urow[2 * p + 1] = 0;
+    un[2 * p + 1] = ly1[p] >= ly0[p] ? ((ly1[p] << sub) >> 2) - ur[2 * p + 1] + 1 : 0;
   }
+  wait_units(c, sm, ur, uc, urow, un);
   __threadfence();
   __syncthreads();
   for (int p = 0; p < 3; p++) {
@@ -840,15 +866,20 @@ __global__ void k_block_map(const FrameParams *fp, const BlockInfo *blocks, cons
   }
 }
 
-// The claim list: every block index, superblocks in wave order and decode
-// order inside each (a prefix sum of the superblocks' block counts over one
-// CTA), and its length.
-__global__ void __launch_bounds__(1024) k_block_order(const SbInfo *sbs, const int *order, int nsb, int *list,
-                                                      int *total) {
+// The claim list of the intra workers: the frame's intra blocks,
+// superblocks in wave order and decode order inside each (a prefix sum of
+// the superblocks' intra block counts over one CTA), and its length.
+__device__ __forceinline__ int intra_count(const BlockInfo *blocks, const SbInfo *sbs, int sb) {
+  int n = imax(0, imin(sbs[sb].num_blocks, MAX_BLOCKS_PER_SB)), m = 0;
+  for (int k = 0; k < n; k++) m += !blocks[sb * MAX_BLOCKS_PER_SB + k].is_inter;
+  return m;
+}
+__global__ void __launch_bounds__(1024) k_block_order(const BlockInfo *blocks, const SbInfo *sbs, const int *order,
+                                                      int nsb, int *list, int *total) {
   __shared__ int part[1024];
   int t = threadIdx.x, per = (nsb + 1023) / 1024, s0 = imin(nsb, t * per), s1 = imin(nsb, s0 + per);
   int sum = 0;
-  for (int i = s0; i < s1; i++) sum += imax(0, imin(sbs[order[i]].num_blocks, MAX_BLOCKS_PER_SB));
+  for (int i = s0; i < s1; i++) sum += intra_count(blocks, sbs, order[i]);
   part[t] = sum;
   __syncthreads();
   for (int off = 1; off < 1024; off <<= 1) {
@@ -860,9 +891,42 @@ __global__ void __launch_bounds__(1024) k_block_order(const SbInfo *sbs, const i
   int base = part[t] - sum;
   for (int i = s0; i < s1; i++) {
     int sb = order[i], n = imax(0, imin(sbs[sb].num_blocks, MAX_BLOCKS_PER_SB));
-    for (int k = 0; k < n; k++) list[base++] = sb * MAX_BLOCKS_PER_SB + k;
+    for (int k = 0; k < n; k++)
+      if (!blocks[sb * MAX_BLOCKS_PER_SB + k].is_inter) list[base++] = sb * MAX_BLOCKS_PER_SB + k;
   }
   if (t == 1023) *total = part[1023];
+}
+
+// The CTA's shared copy of the forward matrices of lengths 4..16.
+__device__ void load_fwd_matrices(const Ctx &c, Smem &sm) {
+  for (int kind = 0; kind < 3; kind++)
+    for (int lg = 2; lg <= 4; lg++) {
+      int n = 1 << (2 * lg), off = lg == 2 ? 0 : lg == 3 ? 16 : 80;
+      for (int k = threadIdx.x; k < n; k += RT) sm.fmat[kind][off + k] = c.mats[fwd_slot(kind, lg) + k];
+    }
+  __syncthreads();
+}
+
+// The inter blocks of the frame, one CTA per superblock (all at once: they
+// read reference pictures only), each published complete for the intra
+// workers that read its samples.
+__global__ void __launch_bounds__(INTER_THREADS) k_recon_inter(Ctx c) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Smem &sm = *(Smem *)smem_raw;
+  int sb = blockIdx.x, n = imax(0, imin(c.sbs[sb].num_blocks, MAX_BLOCKS_PER_SB));
+  load_fwd_matrices(c, sm);
+  for (int k = 0; k < n; k++) {
+    int me = sb * MAX_BLOCKS_PER_SB + k;
+    if (threadIdx.x == 0) sm.blk = c.blocks[me];
+    __syncthreads();
+    if (sm.blk.is_inter) {
+      recon_block(c, sm, c.blocks + me);
+      __threadfence();
+      __syncthreads();
+      if (threadIdx.x == 0) atomicExch(c.done + me, 1);
+    }
+    __syncthreads();
+  }
 }
 
 // Claim state of the recon launch: the list, its length and the counter.
@@ -875,15 +939,11 @@ struct Claim {
 // Every block of the frame, one persistent launch: each CTA (one warp)
 // claims the next block of the list, codes it (waiting inside on the blocks
 // its intra edges read) and publishes its completion flag.
-__global__ void __launch_bounds__(RT, 1) k_recon_blocks(Ctx c, Claim q) {
+__global__ void __launch_bounds__(INTRA_THREADS, 1) k_recon_blocks(Ctx c, Claim q) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Smem &sm = *(Smem *)smem_raw;
   const FrameParams *fp = c.fp;
-  for (int kind = 0; kind < 3; kind++)
-    for (int lg = 2; lg <= 4; lg++) {
-      int n = 1 << (2 * lg), off = lg == 2 ? 0 : lg == 3 ? 16 : 80;
-      for (int k = threadIdx.x; k < n; k += RT) sm.fmat[kind][off + k] = c.mats[fwd_slot(kind, lg) + k];
-    }
+  load_fwd_matrices(c, sm);
   volatile int *vstatus = c.status;
   int total = *q.total;
   for (;;) {

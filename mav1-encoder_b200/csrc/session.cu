@@ -298,11 +298,12 @@ extern "C" int mav1cu_session_create(int width, int height, int max_cdef_presets
     return code;
   }
   cudaFuncSetAttribute(rec::k_recon_blocks, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(rec::Smem));
+  cudaFuncSetAttribute(rec::k_recon_inter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(rec::Smem));
   {
     int dev = 0, sms = 0, per = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, rec::k_recon_blocks, RT, sizeof(rec::Smem));
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, rec::k_recon_blocks, rec::INTRA_THREADS, sizeof(rec::Smem));
     s->resident_recon = imax(1, sms * imax(1, per));
   }
   cudaFuncSetAttribute(ana::k_analyze_level, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -490,24 +491,26 @@ extern "C" int mav1cu_recon(mav1cu_session *s) {
   c.blk_at = s->blk_at;
   c.done = s->blk_done;
   int nsb = s->g.num_sbs;
-  // leaf frames hold inter blocks only (the analysis never keeps intra
-  // there): no intra edge reads, no unit map
-  if (!(s->fp.leaf && !s->fp.frame_is_intra)) {
-    rec::k_block_map<<<(nsb + 3) / 4, 128, 0, s->stream>>>(DP(s), c.blocks, c.sbs, s->blk_at);
-    if (after_launch(s, "recon unit map")) return s->err;
-  }
-  rec::k_block_order<<<1, 1024, 0, s->stream>>>(c.sbs, s->waves, nsb, s->blk_list, s->status + 3);
-  if (after_launch(s, "recon claim list")) return s->err;
   if (check_cuda(s, cudaMemsetAsync(s->blk_done, 0, sizeof(int) * MAX_BLOCKS_PER_SB * nsb, s->stream),
-                 "recon flags") ||
-      check_cuda(s, cudaMemsetAsync(s->status + 2, 0, sizeof(int), s->stream), "recon counter"))
+                 "recon flags"))
     return s->err;
+  if (!s->fp.frame_is_intra) {
+    rec::k_recon_inter<<<nsb, rec::INTER_THREADS, sizeof(rec::Smem), s->stream>>>(c);
+    if (after_launch(s, "recon inter blocks")) return s->err;
+  }
+  // leaf frames code inter blocks only (the analysis never keeps intra there)
+  if (s->fp.leaf && !s->fp.frame_is_intra) return MAV1CU_OK;
+  rec::k_block_map<<<(nsb + 3) / 4, 128, 0, s->stream>>>(DP(s), c.blocks, c.sbs, s->blk_at);
+  if (after_launch(s, "recon unit map")) return s->err;
+  rec::k_block_order<<<1, 1024, 0, s->stream>>>(c.blocks, c.sbs, s->waves, nsb, s->blk_list, s->status + 3);
+  if (after_launch(s, "recon claim list")) return s->err;
+  if (check_cuda(s, cudaMemsetAsync(s->status + 2, 0, sizeof(int), s->stream), "recon counter")) return s->err;
   rec::Claim q;
   q.list = s->blk_list;
   q.total = s->status + 3;
   q.next = s->status + 2;
-  rec::k_recon_blocks<<<s->resident_recon, RT, sizeof(rec::Smem), s->stream>>>(c, q);
-  return after_launch(s, "recon");
+  rec::k_recon_blocks<<<s->resident_recon, rec::INTRA_THREADS, sizeof(rec::Smem), s->stream>>>(c, q);
+  return after_launch(s, "recon intra blocks");
 }
 
 extern "C" int mav1cu_frame_core(mav1cu_session *s) {
