@@ -66,8 +66,9 @@ struct Ctx {
   int *done;            // per block index: 1 once its samples are written
 };
 
-#define TILE_Y 129     // 2 * 64 + 1
-#define TILE_C 65      // 2 * 32 + 1
+#define TILE_OFF 4     // tile column of the block's first sample (word aligned; the left column at 3)
+#define TILE_Y 132     // luma tile stride: TILE_OFF + 2 * 64; rows -1 .. 127
+#define TILE_C 68      // chroma tile stride: TILE_OFF + 2 * 32; rows -1 .. 63
 #define FMAT_SMALL 336 // 4 * 4 + 8 * 8 + 16 * 16
 
 struct Smem {
@@ -91,13 +92,15 @@ struct Smem {
   int rstride[3];
   const uint8_t *srcp[3];
   int sstride[3];
-  int sbBlk[256];            // block index of each 4x4 luma unit of the superblock (-1: outside the frame)
+  FrameParams fpc;           // the CTA's copy of the frame parameters
+  int cornerBlk[6];          // block index at the above-right / below-left corner unit per plane (-1: none)
+  int cornerAR[3], cornerBL[3];  // BlockDecoded of those units
   int32_t fmat[3][FMAT_SMALL];  // forward matrices of lengths 4, 8, 16 per kind
   // intra block tiles: rows and columns -1 .. 2n - 1 around the block (its
   // own samples, the above row over the above-right units, the left column
   // over the below-left units), and its source
-  uint8_t tileY[TILE_Y * TILE_Y];
-  uint8_t tileC[2][TILE_C * TILE_C];
+  uint8_t tileY[TILE_Y * 129];
+  uint8_t tileC[2][TILE_C * 65];
   uint8_t srcY[64 * 64];
   uint8_t srcC[2][32 * 32];
 };
@@ -227,6 +230,33 @@ __device__ __forceinline__ const int32_t *fwd_matrix(const Ctx &c, const Smem &s
   return lg <= 4 ? sm.fmat[kind] + (lg == 2 ? 0 : lg == 3 ? 16 : 80) : c.mats + fwd_slot(kind, lg);
 }
 
+// Forward row pass at a fixed width: row i of the residual (sm.resid,
+// stride 64) times the kept TW rows of the Q20 matrix, 64-bit sums rounded
+// by 16 bits into sm.tmp (stride 32).
+template <int LW>
+__device__ void fwd_rows(Smem &sm, const int32_t *Mh, int h) {
+  constexpr int W = 1 << LW, LTW = LW < 5 ? LW : 5, TW = 1 << LTW;
+  for (int k = threadIdx.x; k < h * TW; k += RT) {
+    int i = k >> LTW, kk = k & (TW - 1);
+    const int32_t *r = sm.resid + i * 64, *m = Mh + kk * W;
+    int64_t s = 0;
+#pragma unroll
+    for (int j = 0; j < W; j++) s += (int64_t)r[j] * m[j];
+    sm.tmp[i * 32 + kk] = (int32_t)round2l(s, 16);
+  }
+}
+
+// Forward column sum at a fixed height for output (k2, kk).
+template <int LH>
+__device__ __forceinline__ int64_t fwd_col(const Smem &sm, const int32_t *Mv, int k2, int kk) {
+  constexpr int H = 1 << LH;
+  const int32_t *m = Mv + k2 * H;
+  int64_t s = 0;
+#pragma unroll
+  for (int i = 0; i < H; i++) s += (int64_t)m[i] * sm.tmp[i * 32 + kk];
+  return s;
+}
+
 // Transform, quantise and reconstruct one transform block whose prediction
 // is in `rec` (code_tx_block, k_recon.h:60-173). Returns the eob.
 __device__ int code_tx(const Ctx &c, Smem &sm, const uint8_t *src, int stride, uint8_t *rec, int rs, int x, int y, int txSz,
@@ -317,21 +347,27 @@ __device__ int code_tx(const Ctx &c, Smem &sm, const uint8_t *src, int stride, u
     }
     __syncthreads();
     const int32_t *Mh = fwd_matrix(c, sm, tx::row_kind(t), lw), *Mv = fwd_matrix(c, sm, tx::col_kind(t), lh);
-    for (int k = tid; k < h * tw; k += RT) {
-      int i = k / tw, kk = k % tw;
-      const int32_t *r = sm.resid + i * 64, *m = Mh + kk * w;
-      int64_t s = 0;
-      for (int j = 0; j < w; j++) s += (int64_t)r[j] * m[j];
-      sm.tmp[i * 32 + kk] = (int32_t)round2l(s, 16);
+    switch (lw) {
+      case 2: fwd_rows<2>(sm, Mh, h); break;
+      case 3: fwd_rows<3>(sm, Mh, h); break;
+      case 4: fwd_rows<4>(sm, Mh, h); break;
+      case 5: fwd_rows<5>(sm, Mh, h); break;
+      default: fwd_rows<6>(sm, Mh, h); break;
     }
     __syncthreads();
     const int16_t *inv = d_inv_scan + d_inv_scan_off[scan_class(t)][txSz];
     int myEob = 0, myNz = 0;
+    int ltw = imin(5, lw);
     for (int k = tid; k < th * tw; k += RT) {
-      int k2 = k / tw, kk = k % tw;
-      const int32_t *m = Mv + k2 * h;
-      int64_t s = 0;
-      for (int i = 0; i < h; i++) s += (int64_t)m[i] * sm.tmp[i * 32 + kk];
+      int k2 = k >> ltw, kk = k & (tw - 1);
+      int64_t s;
+      switch (lh) {
+        case 2: s = fwd_col<2>(sm, Mv, k2, kk); break;
+        case 3: s = fwd_col<3>(sm, Mv, k2, kk); break;
+        case 4: s = fwd_col<4>(sm, Mv, k2, kk); break;
+        case 5: s = fwd_col<5>(sm, Mv, k2, kk); break;
+        default: s = fwd_col<6>(sm, Mv, k2, kk); break;
+      }
       s = s * ((int64_t)1 << shifts);
       if (rect) s = round2l(s, 12) * 5793;
       int v = (int)(s >= 0 ? round2l(s, 20) : -round2l(-s, 20));
@@ -457,36 +493,48 @@ __device__ int cfl_alpha(Smem &sm, const uint8_t *luma, int ls, int startX, int 
   return bestA;
 }
 
+// The clear-flags value of a unit outside the superblock (superblock-relative
+// units of the plane, -1..n): clear_block_decoded_flags (k_recon.h:402-414).
+__device__ __forceinline__ int decoded_outside(const FrameParams *fp, const Smem &sm, int sub, int y, int x) {
+  int n = 16 >> sub;
+  if (y == n && x == -1) return 0;
+  if (y < 0) return x < ((tile_col_end(fp, sm.c0) - sm.c0) >> sub);
+  if (x < 0) return y < ((fp->mi_rows - sm.r0) >> sub);
+  return 0;
+}
+
 // BlockDecoded[plane][y][x] (superblock-relative units of the plane, -1..n)
-// as the reference's flags hold it when block sm.me codes a transform
-// block: outside the superblock, clear_block_decoded_flags' values
-// (k_recon.h:402-414); inside, set by every block before this one in decode
-// order. `own` answers for a unit of this block itself: its transform blocks
+// as the reference's flags hold it when block sm.blk codes a transform
+// block. Outside the superblock: the clear-flags values. Inside, a unit is
+// decoded when the block covering it precedes this one in decode order. The
+// queries (above-right / below-left of a transform block) land on this
+// block itself, directly above it or left of it (blocks there precede it),
+// directly right of it or below it (they follow it), or on the block's
+// above-right / below-left corner unit, looked up once per block in
+// stage_intra. `own` answers for a unit of this block: its transform blocks
 // run in raster order, so the unit above-right of one is coded (1) and the
 // unit below-left is not (0). Units beyond the frame report 0: the edge
 // limits clip to maxX / maxY there, so their flag is never used.
 __device__ int decoded(const Ctx &c, const Smem &sm, int plane, int y, int x, int own) {
   const FrameParams *fp = c.fp;
   int sub = plane > 0, n = 16 >> sub;
-  if (y < 0 || x < 0 || y >= n || x >= n) {
-    if (y == n && x == -1) return 0;
-    if (y < 0) return x < ((tile_col_end(fp, sm.c0) - sm.c0) >> sub);
-    if (x < 0) return y < ((fp->mi_rows - sm.r0) >> sub);
-    return 0;
-  }
+  if (y < 0 || x < 0 || y >= n || x >= n) return decoded_outside(fp, sm, sub, y, x);
   if (sm.r0 + (y << sub) >= fp->mi_rows || sm.c0 + (x << sub) >= fp->mi_cols) return 0;
-  int b = sm.sbBlk[(y << sub) * 16 + (x << sub)];
-  return b == sm.me ? own : (b >= 0 && b < sm.me);
+  const BlockInfo &b = sm.blk;
+  int top = (b.mi_row & 15) >> sub, left = (b.mi_col & 15) >> sub;
+  int bottom = top + (block_h(b.bsize) >> (2 + sub)), right = left + (block_w(b.bsize) >> (2 + sub));
+  if (y >= top && y < bottom && x >= left && x < right) return own;
+  if (y == top - 1 && x == right) return sm.cornerAR[plane];
+  if (y == bottom && x == left - 1) return sm.cornerBL[plane];
+  return y < top || x < left;
 }
 
 #define SPIN_LIMIT (1 << 22)  // polls of at least one L2 round trip each: about a second
 
-// Block index covering 4x4 luma unit (r, col): the superblock's map in
-// shared memory, else the frame's map (neighbouring superblocks).
-__device__ __forceinline__ int block_at(const Ctx &c, const Smem &sm, int r, int col) {
-  int dr = r - sm.r0, dc = col - sm.c0;
-  if ((unsigned)dr < 16u && (unsigned)dc < 16u) return sm.sbBlk[dr * 16 + dc];
-  return c.blk_at[r * c.fp->mi_cols + col];
+// Block index covering 4x4 luma unit (r, col) (the frame's map, built
+// before the launch).
+__device__ __forceinline__ int block_at(const Ctx &c, const Smem &, int r, int col) {
+  return __ldg(c.blk_at + r * c.fp->mi_cols + col);
 }
 
 // Waits until the block covering each 4x4 unit of up to 6 runs of units
@@ -520,40 +568,108 @@ __device__ void wait_units(const Ctx &c, const Smem &sm, const int *r, const int
   }
 }
 
-// Stages an intra block in shared memory: the superblock's unit map, the
-// block's own samples of every plane (the reconstruction so far, overwritten
-// as it is coded) and its source; then, once the blocks that wrote them are
-// complete, the edge samples its transform blocks can read. Those are the
-// row above and the column left of the block, extended past its corner by
-// the largest candidate transform's shorter side where the above-right /
-// below-left unit is decoded: the union of the samples intra_edges reads
-// (above / left limits, spec 7.11.2) over every transform block of every
-// candidate size. The views then point at the tiles.
+// A run of 32-bit words to copy from global to shared memory: n words,
+// 2^lgw per row, row strides gs (global) / ds (shared) bytes.
+struct CopySeg {
+  uint8_t *dst;
+  const uint8_t *src;
+  int ds, gs, n, lgw;
+};
+
+// Copies up to NS runs at once through L2 (__ldcg: the frame is being
+// written by other SMs): each lane issues the loads of a batch of words
+// from any of the runs before its stores, so the whole copy costs about one
+// L2 round trip per batch.
+#define COPY_BATCH 8
+template <int NS>
+__device__ void copy_segs(const CopySeg *sg) {
+  int total = 0;
+#pragma unroll
+  for (int k = 0; k < NS; k++) total += sg[k].n;
+  for (int base = 0; base < total; base += RT * COPY_BATCH) {
+    uint32_t v[COPY_BATCH];
+    uint32_t *d[COPY_BATCH];
+#pragma unroll
+    for (int m = 0; m < COPY_BATCH; m++) {
+      int j = base + m * RT + (int)threadIdx.x, k = 0;
+      d[m] = nullptr;
+      if (j >= total) continue;
+#pragma unroll
+      for (int q = 0; q < NS - 1; q++)
+        if (k == q && j >= sg[q].n) {
+          j -= sg[q].n;
+          k = q + 1;
+        }
+      const CopySeg &g = sg[k];
+      int r = j >> g.lgw, w = j & ((1 << g.lgw) - 1);
+      v[m] = __ldcg((const unsigned *)(g.src + r * g.gs + 4 * w));
+      d[m] = (uint32_t *)(g.dst + r * g.ds + 4 * w);
+    }
+#pragma unroll
+    for (int m = 0; m < COPY_BATCH; m++)
+      if (d[m]) *d[m] = v[m];
+  }
+}
+
+// Stages an intra block in shared memory: the block's own samples of every
+// plane (the reconstruction so far, overwritten as it is coded), its source
+// and its corner units' block indices; then, once the blocks that wrote
+// them are complete, the edge samples its transform blocks can read. Those
+// are the row above and the column left of the block, extended past its
+// corner by the largest candidate transform's shorter side where the
+// above-right / below-left unit is decoded: the union of the samples
+// intra_edges reads (above / left limits, spec 7.11.2) over every transform
+// block of every candidate size. Copies move whole aligned words (a word of
+// the row above or of the column left may carry samples no transform block
+// reads). The views then point at the tiles.
 __device__ void stage_intra(const Ctx &c, Smem &sm) {
   const FrameParams *fp = c.fp;
   const BlockInfo &b = sm.blk;
   int bs = b.bsize, tid = threadIdx.x;
-  for (int k = tid; k < 256; k += RT) {
-    int r = sm.r0 + (k >> 4), col = sm.c0 + (k & 15);
-    sm.sbBlk[k] = (r < fp->mi_rows && col < fp->mi_cols) ? c.blk_at[r * fp->mi_cols + col] : -1;
-  }
+  CopySeg sg[12];
+  int ns = 0;
   for (int p = 0; p < 3; p++) {
     int sub = p > 0, S = sub ? TILE_C : TILE_Y;
     uint8_t *t = sub ? sm.tileC[p - 1] : sm.tileY, *sb = sub ? sm.srcC[p - 1] : sm.srcY;
     int lw = floor_log2(block_w(bs) >> sub), w = 1 << lw, h = block_h(bs) >> sub;
     int x0 = (b.mi_col >> sub) * 4, y0 = (b.mi_row >> sub) * 4, fs = fp->stride[p];
-    const uint8_t *g = c.rec + fp->offset[p], *sp = c.src + fp->offset[p];
-    for (int k = tid; k < w * h; k += RT) {
-      int i = k >> lw, j = k & (w - 1);
-      t[(i + 1) * S + j + 1] = (uint8_t)ldpx(g + (y0 + i) * fs + x0 + j);
-      sb[k] = sp[(y0 + i) * fs + x0 + j];
+    sg[ns++] = CopySeg{t + S + TILE_OFF, c.rec + fp->offset[p] + y0 * fs + x0, S, fs, (w >> 2) * h, lw - 2};
+    sg[ns++] = CopySeg{sb, c.src + fp->offset[p] + y0 * fs + x0, w, fs, (w >> 2) * h, lw - 2};
+    // the corner units: above-right (top - 1, right), below-left (bottom, left - 1)
+    int top = (b.mi_row & 15) >> sub, left = (b.mi_col & 15) >> sub, n = 16 >> sub;
+    int bottom = top + (h >> 2), right = left + (w >> 2);
+    for (int k = 0; k < 2; k++) {
+      int y = k ? bottom : top - 1, x = k ? left - 1 : right;
+      int r = sm.r0 + (y << sub), col = sm.c0 + (x << sub);
+      int inside = y >= 0 && x >= 0 && y < n && x < n && r < fp->mi_rows && col < fp->mi_cols;
+      if (tid == 0) sm.cornerBlk[2 * p + k] = -1;
+      sg[ns++] = CopySeg{(uint8_t *)&sm.cornerBlk[2 * p + k], (const uint8_t *)(c.blk_at + r * fp->mi_cols + col), 0, 0,
+                         inside, 0};
     }
     if (tid == 0) {
-      sm.recp[p] = t + S + 1 - ((ptrdiff_t)y0 * S + x0);
+      sm.recp[p] = t + S + TILE_OFF - ((ptrdiff_t)y0 * S + x0);
       sm.rstride[p] = S;
       sm.srcp[p] = sb - ((ptrdiff_t)y0 * w + x0);
       sm.sstride[p] = w;
     }
+  }
+  __syncwarp();
+  __syncthreads();
+  copy_segs<12>(sg);
+  __syncthreads();
+  if (tid < 6) {
+    int p = tid >> 1, k = tid & 1, sub = p > 0, n = 16 >> sub;
+    int h = block_h(bs) >> sub, w = block_w(bs) >> sub;
+    int top = (b.mi_row & 15) >> sub, left = (b.mi_col & 15) >> sub;
+    int y = k ? top + (h >> 2) : top - 1, x = k ? left - 1 : left + (w >> 2);
+    int v;
+    if (y < 0 || x < 0 || y >= n || x >= n) v = decoded_outside(fp, sm, sub, y, x);
+    else {
+      int blk = sm.cornerBlk[tid];
+      v = blk >= 0 && blk < sm.me;  // -1: beyond the frame
+    }
+    if (k) sm.cornerBL[p] = v;
+    else sm.cornerAR[p] = v;
   }
   __syncthreads();
   int availU = b.mi_row > 0, availL = b.mi_col > tile_col_start(fp, b.mi_col);
@@ -564,8 +680,7 @@ __device__ void stage_intra(const Ctx &c, Smem &sm) {
     int x0 = (b.mi_col >> sub) * 4, y0 = (b.mi_row >> sub) * 4;
     int txSz = fp->lossless ? TX_4X4 : sub ? uv_tx_size(bs, 1, 1) : T(Max_Tx_Size_Rect)[bs];
     int ext = imin(T(Tx_Width)[txSz], T(Tx_Height)[txSz]);
-    int rowU = (b.mi_row & 15) >> sub, colU = (b.mi_col & 15) >> sub;
-    int ar = decoded(c, sm, p, rowU - 1, colU + (w >> 2), 0), bl = decoded(c, sm, p, rowU + (h >> 2), colU - 1, 0);
+    int ar = sm.cornerAR[p], bl = sm.cornerBL[p];
     int maxX = ((fp->mi_cols * 4) >> sub) - 1, maxY = ((fp->mi_rows * 4) >> sub) - 1;
     ay[p] = y0 - 1;
     ax0[p] = x0 - availL;
@@ -584,32 +699,37 @@ __device__ void stage_intra(const Ctx &c, Smem &sm) {
   wait_units(c, sm, ur, uc, urow, un);
   __threadfence();
   __syncthreads();
+  ns = 0;
   for (int p = 0; p < 3; p++) {
     int sub = p > 0, S = sub ? TILE_C : TILE_Y;
     uint8_t *t = sub ? sm.tileC[p - 1] : sm.tileY;
     int x0 = (b.mi_col >> sub) * 4, y0 = (b.mi_row >> sub) * 4, fs = fp->stride[p];
     const uint8_t *g = c.rec + fp->offset[p];
-    for (int k = tid; k <= ax1[p] - ax0[p]; k += RT)
-      t[ax0[p] - x0 + 1 + k] = (uint8_t)ldpx(g + ay[p] * fs + ax0[p] + k);
-    for (int k = tid; k <= ly1[p] - ly0[p]; k += RT)
-      t[(ly0[p] - y0 + 1 + k) * S] = (uint8_t)ldpx(g + (ly0[p] + k) * fs + x0 - 1);
+    int xs = ax0[p] & ~3;  // the row above, from the word holding its first sample
+    sg[ns++] = CopySeg{t + xs - x0 + TILE_OFF, g + ay[p] * fs + xs, 0, 0,
+                       ax1[p] >= ax0[p] ? ((ax1[p] - xs) >> 2) + 1 : 0, 20};
+    // the column left: the word ending at it, one per row
+    sg[ns++] = CopySeg{t + (ly0[p] - y0 + 1) * S + TILE_OFF - 4, g + ly0[p] * fs + x0 - 4, S, fs,
+                       ly1[p] >= ly0[p] ? ly1[p] - ly0[p] + 1 : 0, 0};
   }
+  copy_segs<6>(sg);
   __syncthreads();
 }
 
-// Writes an intra block's own samples from its tiles to the frame.
+// Writes an intra block's own samples from its tiles to the frame (whole
+// words: block positions and widths are multiples of 4 samples).
 __device__ void unstage_intra(const Ctx &c, Smem &sm) {
   const FrameParams *fp = c.fp;
   const BlockInfo &b = sm.blk;
   for (int p = 0; p < 3; p++) {
     int sub = p > 0, S = sub ? TILE_C : TILE_Y;
     const uint8_t *t = sub ? sm.tileC[p - 1] : sm.tileY;
-    int lw = floor_log2(block_w(b.bsize) >> sub), w = 1 << lw, h = block_h(b.bsize) >> sub;
+    int lw = floor_log2(block_w(b.bsize) >> sub) - 2, h = block_h(b.bsize) >> sub;
     int x0 = (b.mi_col >> sub) * 4, y0 = (b.mi_row >> sub) * 4, fs = fp->stride[p];
-    uint8_t *g = c.rec + fp->offset[p];
-    for (int k = threadIdx.x; k < w * h; k += RT) {
-      int i = k >> lw, j = k & (w - 1);
-      g[(y0 + i) * fs + x0 + j] = t[(i + 1) * S + j + 1];
+    uint8_t *g = c.rec + fp->offset[p] + y0 * fs + x0;
+    for (int k = threadIdx.x; k < (h << lw); k += RT) {
+      int i = k >> lw, j = k & ((1 << lw) - 1);
+      *(uint32_t *)(g + i * fs + 4 * j) = *(const uint32_t *)(t + (i + 1) * S + TILE_OFF + 4 * j);
     }
   }
 }
@@ -897,24 +1017,31 @@ __global__ void __launch_bounds__(1024) k_block_order(const BlockInfo *blocks, c
   if (t == 1023) *total = part[1023];
 }
 
-// The CTA's shared copy of the forward matrices of lengths 4..16.
-__device__ void load_fwd_matrices(const Ctx &c, Smem &sm) {
+// The CTA's shared copies of the frame parameters and of the forward
+// matrices of lengths 4..16; returns the context reading them.
+__device__ Ctx load_shared(const Ctx &c, Smem &sm) {
+  const int *src = (const int *)c.fp;
+  int *dst = (int *)&sm.fpc;
+  for (int k = threadIdx.x; k < (int)(sizeof(FrameParams) / 4); k += RT) dst[k] = src[k];
+  Ctx cs = c;
+  cs.fp = &sm.fpc;
   for (int kind = 0; kind < 3; kind++)
     for (int lg = 2; lg <= 4; lg++) {
       int n = 1 << (2 * lg), off = lg == 2 ? 0 : lg == 3 ? 16 : 80;
       for (int k = threadIdx.x; k < n; k += RT) sm.fmat[kind][off + k] = c.mats[fwd_slot(kind, lg) + k];
     }
   __syncthreads();
+  return cs;
 }
 
 // The inter blocks of the frame, one CTA per superblock (all at once: they
 // read reference pictures only), each published complete for the intra
 // workers that read its samples.
-__global__ void __launch_bounds__(INTER_THREADS) k_recon_inter(Ctx c) {
+__global__ void __launch_bounds__(INTER_THREADS) k_recon_inter(Ctx cg) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Smem &sm = *(Smem *)smem_raw;
+  const Ctx c = load_shared(cg, sm);
   int sb = blockIdx.x, n = imax(0, imin(c.sbs[sb].num_blocks, MAX_BLOCKS_PER_SB));
-  load_fwd_matrices(c, sm);
   for (int k = 0; k < n; k++) {
     int me = sb * MAX_BLOCKS_PER_SB + k;
     if (threadIdx.x == 0) sm.blk = c.blocks[me];
@@ -939,11 +1066,11 @@ struct Claim {
 // Every block of the frame, one persistent launch: each CTA (one warp)
 // claims the next block of the list, codes it (waiting inside on the blocks
 // its intra edges read) and publishes its completion flag.
-__global__ void __launch_bounds__(INTRA_THREADS, 1) k_recon_blocks(Ctx c, Claim q) {
+__global__ void __launch_bounds__(INTRA_THREADS, 1) k_recon_blocks(Ctx cg, Claim q) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Smem &sm = *(Smem *)smem_raw;
+  const Ctx c = load_shared(cg, sm);
   const FrameParams *fp = c.fp;
-  load_fwd_matrices(c, sm);
   volatile int *vstatus = c.status;
   int total = *q.total;
   for (;;) {
