@@ -36,9 +36,9 @@
 namespace rec {
 
 // Threads of the CTA coding a block: INTER_THREADS for the inter blocks of a
-// superblock, INTRA_THREADS (one warp) for an intra block worker.
+// superblock, INTRA_THREADS for an intra block worker.
 #define RT ((int)blockDim.x)
-constexpr int INTER_THREADS = 256, INTRA_THREADS = 32;
+constexpr int INTER_THREADS = 256, INTRA_THREADS = 128;
 #define FWD_SLOT_SIZE 4096
 HD int fwd_slot(int kind, int log2n) { return (kind * 5 + log2n - 2) * FWD_SLOT_SIZE; }
 
