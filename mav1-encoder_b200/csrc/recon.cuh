@@ -63,7 +63,7 @@ struct Ctx {
   const int32_t *mats;
   int *status;          // [0] error code, [1] abort
   const int *blk_at;    // per 4x4 luma unit of the frame: index of the block covering it
-  int *done;            // per block index: 1 once its samples are written
+  int *done;            // per block index: 1 once its luma samples are written; then the same for chroma
 };
 
 #define TILE_OFF 4     // tile column of the block's first sample (word aligned; the left column at 3)
@@ -511,7 +511,7 @@ __device__ __forceinline__ int decoded_outside(const FrameParams *fp, const Smem
 // block itself, directly above it or left of it (blocks there precede it),
 // directly right of it or below it (they follow it), or on the block's
 // above-right / below-left corner unit, looked up once per block in
-// stage_intra. `own` answers for a unit of this block: its transform blocks
+// stage_begin. `own` answers for a unit of this block: its transform blocks
 // run in raster order, so the unit above-right of one is coded (1) and the
 // unit below-left is not (0). Units beyond the frame report 0: the edge
 // limits clip to maxX / maxY there, so their flag is never used.
@@ -538,16 +538,18 @@ __device__ __forceinline__ int block_at(const Ctx &c, const Smem &, int r, int c
 }
 
 // Waits until the block covering each 4x4 unit of up to 6 runs of units
+// has completed the planes of `group` (0: luma, 1: chroma)
 // (run k: first (r[k], col[k]), along a row if row[k], else a column;
-// n[k] units) is complete, unless it is this block. Lanes take units of
+// n[k] units), unless it is this block. Lanes take units of
 // all runs at once. Every block waited on precedes this one in the claim
 // order (or is an inter block, complete before the launch), so the wait
 // ends; past the limit it sets the error and abort words and gives up,
 // and every other wait then stops too.
-__device__ void wait_units(const Ctx &c, const Smem &sm, const int *r, const int *col, const int *row, const int *n) {
-  volatile const int *vdone = c.done;
-  volatile int *vstatus = c.status;
+__device__ void wait_units(const Ctx &c, const Smem &sm, int group, const int *r, const int *col, const int *row,
+                           const int *n) {
   int nblk = c.fp->sb_cols * c.fp->sb_rows * MAX_BLOCKS_PER_SB;
+  volatile const int *vdone = c.done + group * nblk;
+  volatile int *vstatus = c.status;
   int total = n[0] + n[1] + n[2] + n[3] + n[4] + n[5];
   for (int i = threadIdx.x; i < total; i += RT) {
     int k = 0, j = i;
@@ -611,18 +613,11 @@ __device__ void copy_segs(const CopySeg *sg) {
   }
 }
 
-// Stages an intra block in shared memory: the block's own samples of every
-// plane (the reconstruction so far, overwritten as it is coded), its source
-// and its corner units' block indices; then, once the blocks that wrote
-// them are complete, the edge samples its transform blocks can read. Those
-// are the row above and the column left of the block, extended past its
-// corner by the largest candidate transform's shorter side where the
-// above-right / below-left unit is decoded: the union of the samples
-// intra_edges reads (above / left limits, spec 7.11.2) over every transform
-// block of every candidate size. Copies move whole aligned words (a word of
-// the row above or of the column left may carry samples no transform block
-// reads). The views then point at the tiles.
-__device__ void stage_intra(const Ctx &c, Smem &sm) {
+// Stages an intra block in shared memory, first part: the block's own
+// samples of every plane (the reconstruction so far, overwritten as it is
+// coded), its source and its corner units' block indices, in one batch of
+// copies; the views then point at the tiles.
+__device__ void stage_begin(const Ctx &c, Smem &sm) {
   const FrameParams *fp = c.fp;
   const BlockInfo &b = sm.blk;
   int bs = b.bsize, tid = threadIdx.x;
@@ -653,7 +648,6 @@ __device__ void stage_intra(const Ctx &c, Smem &sm) {
       sm.sstride[p] = w;
     }
   }
-  __syncwarp();
   __syncthreads();
   copy_segs<12>(sg);
   __syncthreads();
@@ -663,8 +657,9 @@ __device__ void stage_intra(const Ctx &c, Smem &sm) {
     int top = (b.mi_row & 15) >> sub, left = (b.mi_col & 15) >> sub;
     int y = k ? top + (h >> 2) : top - 1, x = k ? left - 1 : left + (w >> 2);
     int v;
-    if (y < 0 || x < 0 || y >= n || x >= n) v = decoded_outside(fp, sm, sub, y, x);
-    else {
+    if (y < 0 || x < 0 || y >= n || x >= n) {
+      v = decoded_outside(fp, sm, sub, y, x);
+    } else {
       int blk = sm.cornerBlk[tid];
       v = blk >= 0 && blk < sm.me;  // -1: beyond the frame
     }
@@ -672,56 +667,76 @@ __device__ void stage_intra(const Ctx &c, Smem &sm) {
     else sm.cornerAR[p] = v;
   }
   __syncthreads();
+}
+
+// Second part, per plane group (0: luma, 1: both chroma planes): once the
+// blocks that wrote them have completed those planes, the edge samples the
+// group's transform blocks can read. Those are the row above and the
+// column left of the block, extended past its corner by the largest
+// candidate transform's shorter side where the above-right / below-left
+// unit is decoded: the union of the samples intra_edges reads (above / left
+// limits, spec 7.11.2) over every transform block of every candidate size.
+// Copies move whole aligned words (a word of the row above or of the
+// column left may carry samples no transform block reads).
+__device__ void stage_edges(const Ctx &c, Smem &sm, int group) {
+  const FrameParams *fp = c.fp;
+  const BlockInfo &b = sm.blk;
+  int bs = b.bsize, p0 = group ? 1 : 0, np = group ? 2 : 1;
   int availU = b.mi_row > 0, availL = b.mi_col > tile_col_start(fp, b.mi_col);
-  int ay[3], ax0[3], ax1[3], ly0[3], ly1[3];
-  int ur[6], uc[6], urow[6], un[6];  // the 4x4 luma units under the edge samples
-  for (int p = 0; p < 3; p++) {
-    int sub = p > 0, w = block_w(bs) >> sub, h = block_h(bs) >> sub;
+  int ay[2], ax0[2], ax1[2], ly0[2], ly1[2];
+  int ur[6] = {0}, uc[6] = {0}, urow[6] = {0}, un[6] = {0};  // the 4x4 luma units under the edge samples
+  for (int q = 0; q < np; q++) {
+    int p = p0 + q, sub = p > 0, w = block_w(bs) >> sub, h = block_h(bs) >> sub;
     int x0 = (b.mi_col >> sub) * 4, y0 = (b.mi_row >> sub) * 4;
     int txSz = fp->lossless ? TX_4X4 : sub ? uv_tx_size(bs, 1, 1) : T(Max_Tx_Size_Rect)[bs];
     int ext = imin(T(Tx_Width)[txSz], T(Tx_Height)[txSz]);
     int ar = sm.cornerAR[p], bl = sm.cornerBL[p];
     int maxX = ((fp->mi_cols * 4) >> sub) - 1, maxY = ((fp->mi_rows * 4) >> sub) - 1;
-    ay[p] = y0 - 1;
-    ax0[p] = x0 - availL;
-    ax1[p] = availU ? imin(maxX, x0 + w - 1 + (ar ? ext : 0)) : ax0[p] - 1;
-    ly0[p] = y0 - availU;
-    ly1[p] = availL ? imin(maxY, y0 + h - 1 + (bl ? ext : 0)) : ly0[p] - 1;
-    ur[2 * p] = (ay[p] << sub) >> 2;
-    uc[2 * p] = (ax0[p] << sub) >> 2;
-    urow[2 * p] = 1;
-    un[2 * p] = ax1[p] >= ax0[p] ? ((ax1[p] << sub) >> 2) - uc[2 * p] + 1 : 0;
-    ur[2 * p + 1] = (ly0[p] << sub) >> 2;
-    uc[2 * p + 1] = ((x0 - 1) << sub) >> 2;
-    urow[2 * p + 1] = 0;
-    un[2 * p + 1] = ly1[p] >= ly0[p] ? ((ly1[p] << sub) >> 2) - ur[2 * p + 1] + 1 : 0;
+    ay[q] = y0 - 1;
+    ax0[q] = x0 - availL;
+    ax1[q] = availU ? imin(maxX, x0 + w - 1 + (ar ? ext : 0)) : ax0[q] - 1;
+    ly0[q] = y0 - availU;
+    ly1[q] = availL ? imin(maxY, y0 + h - 1 + (bl ? ext : 0)) : ly0[q] - 1;
+    ur[2 * q] = (ay[q] << sub) >> 2;
+    uc[2 * q] = (ax0[q] << sub) >> 2;
+    urow[2 * q] = 1;
+    un[2 * q] = ax1[q] >= ax0[q] ? ((ax1[q] << sub) >> 2) - uc[2 * q] + 1 : 0;
+    ur[2 * q + 1] = (ly0[q] << sub) >> 2;
+    uc[2 * q + 1] = ((x0 - 1) << sub) >> 2;
+    urow[2 * q + 1] = 0;
+    un[2 * q + 1] = ly1[q] >= ly0[q] ? ((ly1[q] << sub) >> 2) - ur[2 * q + 1] + 1 : 0;
   }
-  wait_units(c, sm, ur, uc, urow, un);
+  wait_units(c, sm, group, ur, uc, urow, un);
   __threadfence();
   __syncthreads();
-  ns = 0;
-  for (int p = 0; p < 3; p++) {
-    int sub = p > 0, S = sub ? TILE_C : TILE_Y;
+  CopySeg sg[4];
+  for (int q = 0; q < 2; q++) {
+    if (q >= np) {
+      sg[2 * q] = sg[2 * q + 1] = CopySeg{nullptr, nullptr, 0, 0, 0, 0};
+      continue;
+    }
+    int p = p0 + q, sub = p > 0, S = sub ? TILE_C : TILE_Y;
     uint8_t *t = sub ? sm.tileC[p - 1] : sm.tileY;
     int x0 = (b.mi_col >> sub) * 4, y0 = (b.mi_row >> sub) * 4, fs = fp->stride[p];
     const uint8_t *g = c.rec + fp->offset[p];
-    int xs = ax0[p] & ~3;  // the row above, from the word holding its first sample
-    sg[ns++] = CopySeg{t + xs - x0 + TILE_OFF, g + ay[p] * fs + xs, 0, 0,
-                       ax1[p] >= ax0[p] ? ((ax1[p] - xs) >> 2) + 1 : 0, 20};
+    int xs = ax0[q] & ~3;  // the row above, from the word holding its first sample
+    sg[2 * q] = CopySeg{t + xs - x0 + TILE_OFF, g + ay[q] * fs + xs, 0, 0,
+                        ax1[q] >= ax0[q] ? ((ax1[q] - xs) >> 2) + 1 : 0, 20};
     // the column left: the word ending at it, one per row
-    sg[ns++] = CopySeg{t + (ly0[p] - y0 + 1) * S + TILE_OFF - 4, g + ly0[p] * fs + x0 - 4, S, fs,
-                       ly1[p] >= ly0[p] ? ly1[p] - ly0[p] + 1 : 0, 0};
+    sg[2 * q + 1] = CopySeg{t + (ly0[q] - y0 + 1) * S + TILE_OFF - 4, g + ly0[q] * fs + x0 - 4, S, fs,
+                            ly1[q] >= ly0[q] ? ly1[q] - ly0[q] + 1 : 0, 0};
   }
-  copy_segs<6>(sg);
+  copy_segs<4>(sg);
   __syncthreads();
 }
 
-// Writes an intra block's own samples from its tiles to the frame (whole
-// words: block positions and widths are multiples of 4 samples).
-__device__ void unstage_intra(const Ctx &c, Smem &sm) {
+// Writes planes p0 .. p1 - 1 of an intra block's own samples from its tiles
+// to the frame (whole words: block positions and widths are multiples of 4
+// samples), then publishes them complete (flag group 0: luma, 1: chroma).
+__device__ void unstage_intra(const Ctx &c, Smem &sm, int p0, int p1) {
   const FrameParams *fp = c.fp;
   const BlockInfo &b = sm.blk;
-  for (int p = 0; p < 3; p++) {
+  for (int p = p0; p < p1; p++) {
     int sub = p > 0, S = sub ? TILE_C : TILE_Y;
     const uint8_t *t = sub ? sm.tileC[p - 1] : sm.tileY;
     int lw = floor_log2(block_w(b.bsize) >> sub) - 2, h = block_h(b.bsize) >> sub;
@@ -732,6 +747,9 @@ __device__ void unstage_intra(const Ctx &c, Smem &sm) {
       *(uint32_t *)(g + i * fs + 4 * j) = *(const uint32_t *)(t + (i + 1) * S + TILE_OFF + 4 * j);
     }
   }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) atomicExch(c.done + (p0 ? fp->sb_cols * fp->sb_rows * MAX_BLOCKS_PER_SB : 0) + sm.me, 1);
 }
 
 // Every transform block of one plane of block b (code_plane, k_recon.h:190-291).
@@ -869,7 +887,10 @@ __device__ void recon_block(const Ctx &c, Smem &sm, BlockInfo *gb) {
     sm.sstride[p] = fp->stride[p];
   }
   __syncthreads();
-  if (!b.is_inter) stage_intra(c, sm);
+  if (!b.is_inter) {
+    stage_begin(c, sm);
+    stage_edges(c, sm, 0);
+  }
   int tid = threadIdx.x;
   if (b.is_inter && fp->switchable_interp && !comp) {
     int w = block_w(bs), h = block_h(bs);
@@ -905,6 +926,12 @@ __device__ void recon_block(const Ctx &c, Smem &sm, BlockInfo *gb) {
     __syncthreads();
   }
   for (int plane = 0; plane < 3; plane++) {
+    if (plane == 1 && !b.is_inter) {
+      // luma is final: publish it, so blocks waiting only on it go ahead
+      // while this one codes its chroma
+      unstage_intra(c, sm, 0, 1);
+      stage_edges(c, sm, 1);
+    }
     int sub = plane > 0, stride = fp->stride[plane];
     int baseX = (MiCol >> sub) * 4, baseY = (MiRow >> sub) * 4;
     if (b.is_inter) {
@@ -965,7 +992,7 @@ __device__ void recon_block(const Ctx &c, Smem &sm, BlockInfo *gb) {
     if (tid == 0) b.tx_depth = bestD;
     __syncthreads();
   }
-  if (!b.is_inter) unstage_intra(c, sm);
+  if (!b.is_inter) unstage_intra(c, sm, 1, 3);
   if (tid == 0) *gb = b;
 }
 
@@ -1050,7 +1077,10 @@ __global__ void __launch_bounds__(INTER_THREADS) k_recon_inter(Ctx cg) {
       recon_block(c, sm, c.blocks + me);
       __threadfence();
       __syncthreads();
-      if (threadIdx.x == 0) atomicExch(c.done + me, 1);
+      if (threadIdx.x == 0) {
+        atomicExch(c.done + me, 1);
+        atomicExch(c.done + c.fp->sb_cols * c.fp->sb_rows * MAX_BLOCKS_PER_SB + me, 1);
+      }
     }
     __syncthreads();
   }
@@ -1089,10 +1119,8 @@ __global__ void __launch_bounds__(INTRA_THREADS, 1) k_recon_blocks(Ctx cg, Claim
     __syncthreads();
     int me = sm.flag;
     if (me < 0) return;
-    recon_block(c, sm, c.blocks + me);
-    __threadfence();
+    recon_block(c, sm, c.blocks + me);  // publishes its luma, then its chroma
     __syncthreads();
-    if (threadIdx.x == 0) atomicExch(c.done + me, 1);
   }
 }
 

@@ -68,7 +68,7 @@ struct mav1cu_session {
   int *status;             // device status: [0] error, [1] abort, [2] claim counter, [3] claim list length
   int *blk_at;             // block index per 4x4 luma unit
   int *blk_list;           // recon claim list
-  int *blk_done;           // per-block completion flags of the recon launch
+  int *blk_done;           // per-block completion flags of the recon launch: luma, then chroma
   int resident_recon;      // recon workers (one-warp CTAs) resident at once
   std::vector<int> wave_start, wave_len;
   int wave_tile_w;
@@ -277,7 +277,7 @@ extern "C" int mav1cu_session_create(int width, int height, int max_cdef_presets
   if (e == cudaSuccess) e = cudaMalloc(&s->status, sizeof(int) * 4);
   if (e == cudaSuccess) e = cudaMalloc(&s->blk_at, sizeof(int) * g.mi_rows * g.mi_cols);
   if (e == cudaSuccess) e = cudaMalloc(&s->blk_list, sizeof(int) * MAX_BLOCKS_PER_SB * nsb);
-  if (e == cudaSuccess) e = cudaMalloc(&s->blk_done, sizeof(int) * MAX_BLOCKS_PER_SB * nsb);
+  if (e == cudaSuccess) e = cudaMalloc(&s->blk_done, 2 * sizeof(int) * MAX_BLOCKS_PER_SB * nsb);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->own_stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) {
     snprintf(err, errlen, "device allocation failed: %s", cudaGetErrorString(e));
@@ -491,7 +491,7 @@ extern "C" int mav1cu_recon(mav1cu_session *s) {
   c.blk_at = s->blk_at;
   c.done = s->blk_done;
   int nsb = s->g.num_sbs;
-  if (check_cuda(s, cudaMemsetAsync(s->blk_done, 0, sizeof(int) * MAX_BLOCKS_PER_SB * nsb, s->stream),
+  if (check_cuda(s, cudaMemsetAsync(s->blk_done, 0, 2 * sizeof(int) * MAX_BLOCKS_PER_SB * nsb, s->stream),
                  "recon flags"))
     return s->err;
   if (!s->fp.frame_is_intra) {
