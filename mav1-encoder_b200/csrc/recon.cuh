@@ -753,6 +753,7 @@ __device__ void unstage_intra(const Ctx &c, Smem &sm, int p0, int p1) {
 }
 
 // Every transform block of one plane of block b (code_plane, k_recon.h:190-291).
+template <bool INTER>
 __device__ long long code_plane(const Ctx &c, Smem &sm, int plane, int txSz) {
   const FrameParams *fp = c.fp;
   BlockInfo &b = sm.blk;
@@ -768,7 +769,7 @@ __device__ long long code_plane(const Ctx &c, Smem &sm, int plane, int txSz) {
   int rs = sm.rstride[plane];
   int stepX = T(Tx_Width)[txSz] >> 2, stepY = T(Tx_Height)[txSz] >> 2;
   int cands[16], numCands = 0;
-  int isInter = b.is_inter;
+  const int isInter = INTER;
   if (plane == 0) {
     int set = get_tx_set(txSz, isInter, fp->reduced_tx_set);
     if (!fp->tx_search || set == TX_SET_DCTONLY || fp->lossless) {
@@ -866,12 +867,13 @@ __device__ long long code_plane(const Ctx &c, Smem &sm, int plane, int txSz) {
 }
 
 // One block (recon_block, k_recon.h:293-394); sm.blk holds it.
+template <bool INTER>
 __device__ void recon_block(const Ctx &c, Smem &sm, BlockInfo *gb) {
   const FrameParams *fp = c.fp;
   BlockInfo &b = sm.blk;
   int bs = b.bsize;
-  int comp = b.is_inter && b.ref_frame1 > INTRA_FRAME;
-  const uint8_t *ref = (b.is_inter && b.ref_frame != LAST_FRAME) ? c.gold : c.ref;
+  int comp = INTER && b.ref_frame1 > INTRA_FRAME;
+  const uint8_t *ref = (INTER && b.ref_frame != LAST_FRAME) ? c.gold : c.ref;
   const uint8_t *ref1 = c.gold;
   int MiRow = b.mi_row, MiCol = b.mi_col;
   if (threadIdx.x == 0) {
@@ -879,7 +881,7 @@ __device__ void recon_block(const Ctx &c, Smem &sm, BlockInfo *gb) {
     b.tx_depth = 0;
     b.interp_filter &= 0x30;
   }
-  if (b.is_inter && threadIdx.x < 3) {
+  if (INTER && threadIdx.x < 3) {
     int p = threadIdx.x;
     sm.recp[p] = c.rec + fp->offset[p];
     sm.rstride[p] = fp->stride[p];
@@ -887,12 +889,12 @@ __device__ void recon_block(const Ctx &c, Smem &sm, BlockInfo *gb) {
     sm.sstride[p] = fp->stride[p];
   }
   __syncthreads();
-  if (!b.is_inter) {
+  if (!INTER) {
     stage_begin(c, sm);
     stage_edges(c, sm, 0);
   }
   int tid = threadIdx.x;
-  if (b.is_inter && fp->switchable_interp && !comp) {
+  if (INTER && fp->switchable_interp && !comp) {
     int w = block_w(bs), h = block_h(bs);
     int x0 = MiCol * 4, y0 = MiRow * 4, stride = fp->stride[0], rs = sm.rstride[0];
     uint8_t *px = sm.recp[0] + y0 * rs + x0;
@@ -926,7 +928,7 @@ __device__ void recon_block(const Ctx &c, Smem &sm, BlockInfo *gb) {
     __syncthreads();
   }
   for (int plane = 0; plane < 3; plane++) {
-    if (plane == 1 && !b.is_inter) {
+    if (plane == 1 && !INTER) {
       // luma is final: publish it, so blocks waiting only on it go ahead
       // while this one codes its chroma
       unstage_intra(c, sm, 0, 1);
@@ -934,7 +936,7 @@ __device__ void recon_block(const Ctx &c, Smem &sm, BlockInfo *gb) {
     }
     int sub = plane > 0, stride = fp->stride[plane];
     int baseX = (MiCol >> sub) * 4, baseY = (MiRow >> sub) * 4;
-    if (b.is_inter) {
+    if (INTER) {
       int w = block_w(bs) >> sub, h = block_h(bs) >> sub;
       int rs = sm.rstride[plane];
       uint8_t *d = sm.recp[plane] + baseY * rs + baseX;
@@ -953,16 +955,16 @@ __device__ void recon_block(const Ctx &c, Smem &sm, BlockInfo *gb) {
       __syncthreads();
     }
     if (fp->lossless) {
-      code_plane(c, sm, plane, TX_4X4);
+      code_plane<INTER>(c, sm, plane, TX_4X4);
       continue;
     }
     if (plane > 0) {
-      code_plane(c, sm, plane, uv_tx_size(bs, 1, 1));
+      code_plane<INTER>(c, sm, plane, uv_tx_size(bs, 1, 1));
       continue;
     }
-    int maxDepth = (!b.is_inter && fp->tx_mode_select) ? imin(MAX_TX_DEPTH, T(Max_Tx_Depth)[bs]) : 0;
+    int maxDepth = (!INTER && fp->tx_mode_select) ? imin(MAX_TX_DEPTH, T(Max_Tx_Depth)[bs]) : 0;
     if (maxDepth == 0) {
-      code_plane(c, sm, 0, T(Max_Tx_Size_Rect)[bs]);
+      code_plane<INTER>(c, sm, 0, T(Max_Tx_Size_Rect)[bs]);
       continue;
     }
     // tx_depth RD search: every depth from the same pixels (BlockDecoded
@@ -982,7 +984,7 @@ __device__ void recon_block(const Ctx &c, Smem &sm, BlockInfo *gb) {
         for (int k = tid; k < w * h; k += RT) px[(k / w) * rs + (k % w)] = sm.save[k];
         __syncthreads();
       }
-      long long cst = code_plane(c, sm, 0, depth_tx_size(bs, depth)) + (long long)fp->lambda * 8 * depth;
+      long long cst = code_plane<INTER>(c, sm, 0, depth_tx_size(bs, depth)) + (long long)fp->lambda * 8 * depth;
       if (d <= maxDepth && (best < 0 || cst < best)) {
         best = cst;
         bestD = depth;
@@ -992,7 +994,7 @@ __device__ void recon_block(const Ctx &c, Smem &sm, BlockInfo *gb) {
     if (tid == 0) b.tx_depth = bestD;
     __syncthreads();
   }
-  if (!b.is_inter) unstage_intra(c, sm, 1, 3);
+  if (!INTER) unstage_intra(c, sm, 1, 3);
   if (tid == 0) *gb = b;
 }
 
@@ -1064,7 +1066,7 @@ __device__ Ctx load_shared(const Ctx &c, Smem &sm) {
 // The inter blocks of the frame, one CTA per superblock (all at once: they
 // read reference pictures only), each published complete for the intra
 // workers that read its samples.
-__global__ void __launch_bounds__(INTER_THREADS) k_recon_inter(Ctx cg) {
+__global__ void __launch_bounds__(INTER_THREADS, 2) k_recon_inter(Ctx cg) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Smem &sm = *(Smem *)smem_raw;
   const Ctx c = load_shared(cg, sm);
@@ -1074,7 +1076,7 @@ __global__ void __launch_bounds__(INTER_THREADS) k_recon_inter(Ctx cg) {
     if (threadIdx.x == 0) sm.blk = c.blocks[me];
     __syncthreads();
     if (sm.blk.is_inter) {
-      recon_block(c, sm, c.blocks + me);
+      recon_block<true>(c, sm, c.blocks + me);
       __threadfence();
       __syncthreads();
       if (threadIdx.x == 0) {
@@ -1119,7 +1121,7 @@ __global__ void __launch_bounds__(INTRA_THREADS, 1) k_recon_blocks(Ctx cg, Claim
     __syncthreads();
     int me = sm.flag;
     if (me < 0) return;
-    recon_block(c, sm, c.blocks + me);  // publishes its luma, then its chroma
+    recon_block<false>(c, sm, c.blocks + me);  // publishes its luma, then its chroma
     __syncthreads();
   }
 }
