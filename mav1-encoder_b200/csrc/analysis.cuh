@@ -536,27 +536,47 @@ __global__ void __launch_bounds__(128) k_analyze_level(Ctx c, int level, int slo
   }
 }
 
-// Pass 2: partition decision and block emission, one thread per superblock
-// (k_analysis.h:697-808).
-__global__ void k_analyze_table(Ctx c) {
-  const FrameParams *fp = c.fp;
-  int sbIdx = blockIdx.x * blockDim.x + threadIdx.x;
-  if (sbIdx >= fp->sb_cols * fp->sb_rows) return;
-  int sbRow = sbIdx / fp->sb_cols, sbCol = sbIdx % fp->sb_cols;
+// Pass 2: partition decision and block emission (k_analysis.h:697-808), one
+// warp per superblock. The nodes of a level are independent: lanes take
+// them, bottom-up level by level, with the costs in shared memory. Emission
+// walks the 64 8x8 positions in Z order: each lane finds the blocks its
+// positions emit, a warp prefix sum of their counts and coefficient sizes
+// gives every block its index and coefficient offsets (the serial walk's).
+#define TABLE_WARPS 4
+struct TableMem {
   long long cost[NUM_NODES], noneCost[NUM_NODES];
   int part[NUM_NODES];
+};
+
+__device__ __forceinline__ int warp_excl_scan(int v, int lane, int *total) {
+  int x = v;
+  for (int off = 1; off < 32; off <<= 1) {
+    int y = __shfl_up_sync(0xffffffffu, x, off);
+    if (lane >= off) x += y;
+  }
+  *total = __shfl_sync(0xffffffffu, x, 31);
+  return x - v;
+}
+
+__global__ void __launch_bounds__(32 * TABLE_WARPS) k_analyze_table(Ctx c) {
+  __shared__ TableMem tms[TABLE_WARPS];
+  const FrameParams *fp = c.fp;
+  int lane = threadIdx.x & 31, sbIdx = blockIdx.x * TABLE_WARPS + (threadIdx.x >> 5);
+  if (sbIdx >= fp->sb_cols * fp->sb_rows) return;
+  TableMem &m = tms[threadIdx.x >> 5];
+  int sbRow = sbIdx / fp->sb_cols, sbCol = sbIdx % fp->sb_cols;
   int lam = fp->ac_q[0] / 16;
   const int64_t *tc = c.costs + (long long)sbIdx * A_ITEMS;
   const BlockInfo *ti = c.infos + (long long)sbIdx * A_ITEMS;
   for (int level = 3; level >= 0; level--) {
     int n = 1 << level, size4 = 16 >> level, bSize = level_bsize(level);
-    for (int i = 0; i < n * n; i++) {
+    for (int i = lane; i < n * n; i += 32) {
       int node = node_base(level) + i;
       int r = sbRow * 16 + (i / n) * size4, cc = sbCol * 16 + (i % n) * size4;
-      noneCost[node] = -1;
+      m.noneCost[node] = -1;
       if (r >= fp->mi_rows || cc >= fp->mi_cols) {
-        cost[node] = 0;
-        part[node] = -1;
+        m.cost[node] = 0;
+        m.part[node] = -1;
         continue;
       }
       int halfSz = size4 >> 1;
@@ -565,9 +585,10 @@ __global__ void k_analyze_table(Ctx c) {
       long long bestC = -1;
       int bestP = PARTITION_SPLIT;
       if (level < 3) {
-        long long c0 = cost[cb + ci], c1 = cost[cb + ci + 1], c2 = cost[cb + ci + cn], c3 = cost[cb + ci + cn + 1];
+        long long c0 = m.cost[cb + ci], c1 = m.cost[cb + ci + 1], c2 = m.cost[cb + ci + cn], c3 = m.cost[cb + ci + cn + 1];
         if (c0 >= 0 && c1 >= 0 && c2 >= 0 && c3 >= 0) bestC = c0 + c1 + c2 + c3 + (long long)lam * 16 / 8;
       }
+      long long noneC = -1;
       for (int p = PARTITION_NONE; p <= PARTITION_VERT_4; p++) {
         if (!part_allowed(fp, level, p, hasRows, hasCols)) continue;
         long long pc = 0;
@@ -578,7 +599,7 @@ __global__ void k_analyze_table(Ctx c) {
           if (s < 0) {
             int dr, dc;
             part_block(p, bSize, k, halfSz, &dr, &dc);
-            v = noneCost[cb + ci + (dr ? cn : 0) + (dc ? 1 : 0)];
+            v = m.noneCost[cb + ci + (dr ? cn : 0) + (dc ? 1 : 0)];
           } else {
             v = tc[node * A_SLOTS + s];
           }
@@ -586,65 +607,98 @@ __global__ void k_analyze_table(Ctx c) {
         }
         if (pc < 0) continue;
         pc += (long long)lam * (p == PARTITION_NONE ? 8 : 24) / 8;
-        if (p == PARTITION_NONE) noneCost[node] = pc;
+        if (p == PARTITION_NONE) noneC = pc;
         if (bestC < 0 || pc <= bestC) {
           bestC = pc;
           bestP = p;
         }
       }
-      cost[node] = bestC;
-      part[node] = bestP;
+      m.noneCost[node] = noneC;
+      m.cost[node] = bestC;
+      m.part[node] = bestP;
     }
+    __syncwarp();
   }
   SbInfo *sb = &c.sbs[sbIdx];
-  for (int k = 0; k < NUM_NODES; k++) sb->part[k] = part[k];
-  int count = 0, coefOff = sbIdx * COEFS_PER_SB;
-  for (int z = 0; z < 64; z++) {
-    int zx = 0, zy = 0;
+  for (int k = lane; k < NUM_NODES; k += 32) sb->part[k] = m.part[k];
+  // the blocks each of this lane's two Z positions emits
+  int nbz[2], nodez[2], levz[2], zyz[2], zxz[2], coefz[2];
+  for (int h = 0; h < 2; h++) {
+    int z = lane + 32 * h, zx = 0, zy = 0;
     for (int bb = 0; bb < 3; bb++) {
       zx |= ((z >> (2 * bb)) & 1) << bb;
       zy |= ((z >> (2 * bb + 1)) & 1) << bb;
     }
+    nbz[h] = 0;
+    coefz[h] = 0;
+    zxz[h] = zx;
+    zyz[h] = zy;
     for (int level = 0; level <= 3; level++) {
       int shift = 3 - level, n = 1 << level;
       int node = node_base(level) + (zy >> shift) * n + (zx >> shift);
-      int p = part[node];
+      int p = m.part[node];
       if (p < 0) break;
       if (p == PARTITION_SPLIT) continue;
       if ((zx & ((1 << shift) - 1)) == 0 && (zy & ((1 << shift) - 1)) == 0) {
         int size4 = 16 >> level, halfMi = size4 >> 1;
         int r = sbRow * 16 + (zy >> shift) * size4, cc = sbCol * 16 + (zx >> shift) * size4;
-        int nb = part_count(fp, p, r, cc, halfMi);
+        nbz[h] = part_count(fp, p, r, cc, halfMi);
+        nodez[h] = node;
+        levz[h] = level;
         int cn = n * 2, ci = (zy >> shift) * 2 * cn + (zx >> shift) * 2, cb = level < 3 ? node_base(level + 1) : 0;
-        for (int k = 0; k < nb; k++) {
-          int s = part_slot(p, k);
-          BlockInfo b;
+        for (int k = 0; k < nbz[h]; k++) {
+          int s = part_slot(p, k), bsz;
           if (s < 0) {
             int dr, dc;
             part_block(p, level_bsize(level), k, halfMi, &dr, &dc);
-            b = ti[(cb + ci + (dr ? cn : 0) + (dc ? 1 : 0)) * A_SLOTS];
+            bsz = ti[(cb + ci + (dr ? cn : 0) + (dc ? 1 : 0)) * A_SLOTS].bsize;
           } else {
-            b = ti[node * A_SLOTS + s];
+            bsz = ti[node * A_SLOTS + s].bsize;
           }
-          int w = block_w(b.bsize), h = block_h(b.bsize);
-          b.coef_off[0] = coefOff;
-          coefOff += w * h;
-          b.coef_off[1] = coefOff;
-          coefOff += (w >> 1) * (h >> 1);
-          b.coef_off[2] = coefOff;
-          coefOff += (w >> 1) * (h >> 1);
-          b.eob[0] = b.eob[1] = b.eob[2] = 0;
-          c.blocks[sbIdx * MAX_BLOCKS_PER_SB + count] = b;
-          count++;
+          int w = block_w(bsz), hh = block_h(bsz);
+          coefz[h] += w * hh + 2 * ((w >> 1) * (hh >> 1));
         }
       }
       break;
     }
   }
-  sb->first_block = sbIdx * MAX_BLOCKS_PER_SB;
-  sb->num_blocks = count;
-  sb->sb_row = sbRow;
-  sb->sb_col = sbCol;
+  int t0, t1, c0t, c1t;
+  int base0 = warp_excl_scan(nbz[0], lane, &t0), base1 = t0 + warp_excl_scan(nbz[1], lane, &t1);
+  int cbase0 = warp_excl_scan(coefz[0], lane, &c0t), cbase1 = c0t + warp_excl_scan(coefz[1], lane, &c1t);
+  for (int h = 0; h < 2; h++) {
+    int count = h ? base1 : base0, coefOff = sbIdx * COEFS_PER_SB + (h ? cbase1 : cbase0);
+    if (!nbz[h]) continue;
+    int level = levz[h], node = nodez[h], shift = 3 - level, n = 1 << level, p = m.part[node];
+    int zx = zxz[h], zy = zyz[h], halfMi = (16 >> level) >> 1;
+    int cn = n * 2, ci = (zy >> shift) * 2 * cn + (zx >> shift) * 2, cb = level < 3 ? node_base(level + 1) : 0;
+    for (int k = 0; k < nbz[h]; k++) {
+      int s = part_slot(p, k);
+      BlockInfo b;
+      if (s < 0) {
+        int dr, dc;
+        part_block(p, level_bsize(level), k, halfMi, &dr, &dc);
+        b = ti[(cb + ci + (dr ? cn : 0) + (dc ? 1 : 0)) * A_SLOTS];
+      } else {
+        b = ti[node * A_SLOTS + s];
+      }
+      int w = block_w(b.bsize), hh = block_h(b.bsize);
+      b.coef_off[0] = coefOff;
+      coefOff += w * hh;
+      b.coef_off[1] = coefOff;
+      coefOff += (w >> 1) * (hh >> 1);
+      b.coef_off[2] = coefOff;
+      coefOff += (w >> 1) * (hh >> 1);
+      b.eob[0] = b.eob[1] = b.eob[2] = 0;
+      c.blocks[sbIdx * MAX_BLOCKS_PER_SB + count] = b;
+      count++;
+    }
+  }
+  if (lane == 0) {
+    sb->first_block = sbIdx * MAX_BLOCKS_PER_SB;
+    sb->num_blocks = t0 + t1;
+    sb->sb_row = sbRow;
+    sb->sb_col = sbCol;
+  }
 }
 
 // ---- intra edge filter types (encoder.c:319-346) ------------------------------------

@@ -461,7 +461,7 @@ extern "C" int mav1cu_analyze(mav1cu_session *s) {
     ana::k_analyze_level<<<(unsigned)((items + 3) / 4), 128, 4 * sizeof(ana::WarpMem), s->stream>>>(c, level, slots);
     if (after_launch(s, "analysis pass 1")) return s->err;
   }
-  ana::k_analyze_table<<<(s->g.num_sbs + 63) / 64, 64, 0, s->stream>>>(c);
+  ana::k_analyze_table<<<(s->g.num_sbs + TABLE_WARPS - 1) / TABLE_WARPS, 32 * TABLE_WARPS, 0, s->stream>>>(c);
   return after_launch(s, "analysis pass 2");
 }
 
