@@ -61,6 +61,7 @@ struct Ctx {
   const SbInfo *sbs;
   int32_t *coefs;
   const int32_t *mats;
+  const int32_t *mats_t;  // the same matrices transposed
   int *status;          // [0] error code, [1] abort
   const int *blk_at;    // per 4x4 luma unit of the frame: index of the block covering it
   int *done;            // per block index: 1 once its luma samples are written; then the same for chroma
@@ -96,6 +97,7 @@ struct Smem {
   int cornerBlk[6];          // block index at the above-right / below-left corner unit per plane (-1: none)
   int cornerAR[3], cornerBL[3];  // BlockDecoded of those units
   int32_t fmat[3][FMAT_SMALL];  // forward matrices of lengths 4, 8, 16 per kind
+  int32_t fmatT[3][FMAT_SMALL]; // the same transposed
   // intra block tiles: rows and columns -1 .. 2n - 1 around the block (its
   // own samples, the above row over the above-right units, the left column
   // over the below-left units), and its source
@@ -225,23 +227,36 @@ __device__ void inverse_2d(Smem &sm, const int32_t *q, int txSz, int txType, int
 }
 
 // Forward matrix of a kind and length: lengths 4..16 from the CTA's shared
-// copy, 32 and 64 from the table in global memory.
+// copy, 32 and 64 from the table in global memory; fwd_matrix_t gives the
+// transpose (the row pass reads it along the output index, so the lanes of
+// a warp read consecutive words).
 __device__ __forceinline__ const int32_t *fwd_matrix(const Ctx &c, const Smem &sm, int kind, int lg) {
   return lg <= 4 ? sm.fmat[kind] + (lg == 2 ? 0 : lg == 3 ? 16 : 80) : c.mats + fwd_slot(kind, lg);
 }
+__device__ __forceinline__ const int32_t *fwd_matrix_t(const Ctx &c, const Smem &sm, int kind, int lg) {
+  return lg <= 4 ? sm.fmatT[kind] + (lg == 2 ? 0 : lg == 3 ? 16 : 80) : c.mats_t + fwd_slot(kind, lg);
+}
+
+// The transpose of every forward matrix (slot k: kind k / 5, length 4 << k % 5).
+__global__ void k_transpose_mats(const int32_t *mats, int32_t *matsT) {
+  int slot = blockIdx.x, n = 4 << (slot % 5);
+  const int32_t *m = mats + slot * FWD_SLOT_SIZE;
+  int32_t *t = matsT + slot * FWD_SLOT_SIZE;
+  for (int e = threadIdx.x; e < n * n; e += blockDim.x) t[(e % n) * n + e / n] = m[e];
+}
 
 // Forward row pass at a fixed width: row i of the residual (sm.resid,
-// stride 64) times the kept TW rows of the Q20 matrix, 64-bit sums rounded
-// by 16 bits into sm.tmp (stride 32).
+// stride 64) times the kept TW rows of the Q20 matrix (read from its
+// transpose MhT), 64-bit sums rounded by 16 bits into sm.tmp (stride 32).
 template <int LW>
-__device__ void fwd_rows(Smem &sm, const int32_t *Mh, int h) {
+__device__ void fwd_rows(Smem &sm, const int32_t *MhT, int h) {
   constexpr int W = 1 << LW, LTW = LW < 5 ? LW : 5, TW = 1 << LTW;
   for (int k = threadIdx.x; k < h * TW; k += RT) {
     int i = k >> LTW, kk = k & (TW - 1);
-    const int32_t *r = sm.resid + i * 64, *m = Mh + kk * W;
+    const int32_t *r = sm.resid + i * 64, *m = MhT + kk;
     int64_t s = 0;
 #pragma unroll
-    for (int j = 0; j < W; j++) s += (int64_t)r[j] * m[j];
+    for (int j = 0; j < W; j++) s += (int64_t)r[j] * m[j * W];
     sm.tmp[i * 32 + kk] = (int32_t)round2l(s, 16);
   }
 }
@@ -346,7 +361,7 @@ __device__ int code_tx(const Ctx &c, Smem &sm, const uint8_t *src, int stride, u
       sm.resid[i * 64 + j] = (int)src[(y + yy) * stride + x + xx] - (int)rec[(y + yy) * rs + x + xx];
     }
     __syncthreads();
-    const int32_t *Mh = fwd_matrix(c, sm, tx::row_kind(t), lw), *Mv = fwd_matrix(c, sm, tx::col_kind(t), lh);
+    const int32_t *Mh = fwd_matrix_t(c, sm, tx::row_kind(t), lw), *Mv = fwd_matrix(c, sm, tx::col_kind(t), lh);
     switch (lw) {
       case 2: fwd_rows<2>(sm, Mh, h); break;
       case 3: fwd_rows<3>(sm, Mh, h); break;
@@ -1057,7 +1072,10 @@ __device__ Ctx load_shared(const Ctx &c, Smem &sm) {
   for (int kind = 0; kind < 3; kind++)
     for (int lg = 2; lg <= 4; lg++) {
       int n = 1 << (2 * lg), off = lg == 2 ? 0 : lg == 3 ? 16 : 80;
-      for (int k = threadIdx.x; k < n; k += RT) sm.fmat[kind][off + k] = c.mats[fwd_slot(kind, lg) + k];
+      for (int k = threadIdx.x; k < n; k += RT) {
+        sm.fmat[kind][off + k] = c.mats[fwd_slot(kind, lg) + k];
+        sm.fmatT[kind][off + k] = c.mats_t[fwd_slot(kind, lg) + k];
+      }
     }
   __syncthreads();
   return cs;

@@ -64,6 +64,9 @@ struct mav1cu_session {
   uint8_t *qp[2];          // 16 quarter-pel planes per reference
   uint8_t *dsrc, *dref[2]; // decimated planes
   uint8_t *ys, *uvs;       // edge-type marks per mi
+  int32_t *mats_t;         // MATS with every matrix transposed (row passes read it along the output index)
+  int mats_dirty;          // MATS changed since mats_t was derived
+  int mats_exposed;        // MATS's device address was handed out: derive mats_t before every recon
   int *waves;              // superblocks in wave order
   int *status;             // device status: [0] error, [1] abort, [2] claim counter, [3] claim list length
   int *blk_at;             // block index per 4x4 luma unit
@@ -228,7 +231,7 @@ static void free_all(mav1cu_session *s) {
   for (int i = 0; i < MAV1CU_BUF_COUNT; i++)
     if (s->buf[i]) cudaFree(s->buf[i]);
   void *extra[] = {s->qp[0], s->qp[1], s->dsrc, s->dref[0], s->dref[1], s->ys, s->uvs, s->waves, s->status, s->blk_at, s->blk_list,
-                   s->blk_done};
+                   s->blk_done, s->mats_t};
   for (void *p : extra)
     if (p) cudaFree(p);
   if (s->own_stream) cudaStreamDestroy(s->own_stream);
@@ -276,6 +279,8 @@ extern "C" int mav1cu_session_create(int width, int height, int max_cdef_presets
   if (e == cudaSuccess) e = cudaMalloc(&s->waves, sizeof(int) * nsb);
   if (e == cudaSuccess) e = cudaMalloc(&s->status, sizeof(int) * 4);
   if (e == cudaSuccess) e = cudaMalloc(&s->blk_at, sizeof(int) * g.mi_rows * g.mi_cols);
+  if (e == cudaSuccess) e = cudaMalloc(&s->mats_t, sizeof(int32_t) * 4096 * 15);
+  s->mats_dirty = 1;
   if (e == cudaSuccess) e = cudaMalloc(&s->blk_list, sizeof(int) * MAX_BLOCKS_PER_SB * nsb);
   if (e == cudaSuccess) e = cudaMalloc(&s->blk_done, 2 * sizeof(int) * MAX_BLOCKS_PER_SB * nsb);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->own_stream, cudaStreamNonBlocking);
@@ -329,6 +334,7 @@ extern "C" size_t mav1cu_buf_size(const mav1cu_session *s, int buf) {
   return buf >= 0 && buf < MAV1CU_BUF_COUNT ? s->size[buf] : 0;
 }
 extern "C" void *mav1cu_buf_device(mav1cu_session *s, int buf) {
+  if (buf == MAV1CU_BUF_MATS) s->mats_exposed = 1;
   return buf >= 0 && buf < MAV1CU_BUF_COUNT ? s->buf[buf] : NULL;
 }
 
@@ -336,6 +342,7 @@ extern "C" int mav1cu_upload(mav1cu_session *s, int buf, const void *host, size_
   if (s->err) return s->err;
   if (buf < 0 || buf >= MAV1CU_BUF_COUNT || bytes > s->size[buf])
     return set_error(s, MAV1CU_ERR_ARG, "upload: buffer %d, %zu bytes", buf, bytes);
+  if (buf == MAV1CU_BUF_MATS) s->mats_dirty = 1;
   return check_cuda(s, cudaMemcpyAsync(s->buf[buf], host, bytes, cudaMemcpyHostToDevice, s->stream), "upload");
 }
 
@@ -351,6 +358,7 @@ extern "C" int mav1cu_copy(mav1cu_session *s, int dst, int src, size_t bytes) {
   if (dst < 0 || dst >= MAV1CU_BUF_COUNT || src < 0 || src >= MAV1CU_BUF_COUNT || bytes > s->size[dst] ||
       bytes > s->size[src])
     return set_error(s, MAV1CU_ERR_ARG, "copy: buffers %d <- %d, %zu bytes", dst, src, bytes);
+  if (dst == MAV1CU_BUF_MATS) s->mats_dirty = 1;
   return check_cuda(s, cudaMemcpyAsync(s->buf[dst], s->buf[src], bytes, cudaMemcpyDeviceToDevice, s->stream), "copy");
 }
 
@@ -487,6 +495,12 @@ extern "C" int mav1cu_recon(mav1cu_session *s) {
   c.sbs = (const SbInfo *)s->buf[MAV1CU_BUF_SBS];
   c.coefs = (int32_t *)s->buf[MAV1CU_BUF_COEFS];
   c.mats = (const int32_t *)s->buf[MAV1CU_BUF_MATS];
+  c.mats_t = s->mats_t;
+  if (s->mats_dirty || s->mats_exposed) {
+    rec::k_transpose_mats<<<15, 256, 0, s->stream>>>(c.mats, s->mats_t);
+    if (after_launch(s, "forward matrices")) return s->err;
+    s->mats_dirty = 0;
+  }
   c.status = s->status;
   c.blk_at = s->blk_at;
   c.done = s->blk_done;
