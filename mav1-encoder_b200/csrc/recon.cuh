@@ -79,6 +79,7 @@ struct Smem {
   int32_t qbest[32 * 32];  // levels kept by the tx type search
   int edge[3][EDGE_LEN];   // AboveRow, LeftCol, filter copy
   uint8_t save[64 * 64];
+  int16_t pred0[64 * 64];  // first compound prediction (intermediate precision)
   int sse33[33];
   long long red[INTER_THREADS / 32];
   BlockInfo blk;
@@ -881,6 +882,44 @@ __device__ long long code_plane(const Ctx &c, Smem &sm, int plane, int txSz) {
   return total;
 }
 
+// Inter prediction of a w x h block (spec 7.11.3.4), staged: the clamped
+// reference window (h + 7 rows of w + 7 samples) in shared memory, the
+// horizontal 8-tap pass of every window row (Round2 by InterRound0 = 3), then
+// the vertical pass per output sample - the values inter_sum forms sample
+// by sample (k_inter.h:451-504). mode 0: final samples (Round2 by 11,
+// clipped) into d (stride ds); 1: compound intermediates (Round2 by 7) into
+// sm.pred0; 2: Round2(pred0 + this block's intermediates, 5), clipped, into
+// d. Scratch: sm.tmp (window), sm.resid (horizontal pass).
+__device__ void predict_block(Smem &sm, const pred::Inter &ip, int lw, int h, int mode, uint8_t *d, int ds) {
+  int w = 1 << lw, W = w + 7, H = h + 7;
+  uint8_t *win = (uint8_t *)sm.tmp;
+  int16_t *hs = (int16_t *)sm.resid;
+  for (int k = threadIdx.x; k < W * H; k += RT) {
+    int R = k / W, C = k - R * W;
+    win[k] = ip.ref[(size_t)clip3(0, ip.lastY, ip.iy0 + R) * ip.stride + clip3(0, ip.lastX, ip.ix0 + C)];
+  }
+  __syncthreads();
+  for (int k = threadIdx.x; k < H * w; k += RT) {
+    int R = k >> lw, cc = k & (w - 1);
+    const uint8_t *row = win + R * W + cc;
+    int s = 0;
+#pragma unroll
+    for (int t = 0; t < 8; t++) s += ip.fh[t] * (int)row[t];
+    hs[k] = (int16_t)round2(s, 3);
+  }
+  __syncthreads();
+  for (int k = threadIdx.x; k < h * w; k += RT) {
+    int r = k >> lw, cc = k & (w - 1);
+    int acc = 0;
+#pragma unroll
+    for (int tv = 0; tv < 8; tv++) acc += ip.fv[tv] * (int)hs[(r + tv) * w + cc];
+    if (mode == 0) d[r * ds + cc] = (uint8_t)clip1(round2(acc, 11));
+    else if (mode == 1) sm.pred0[k] = (int16_t)round2(acc, 7);
+    else d[r * ds + cc] = (uint8_t)clip1(round2((int)sm.pred0[k] + round2(acc, 7), 5));
+  }
+  __syncthreads();
+}
+
 // One block (recon_block, k_recon.h:293-394); sm.blk holds it.
 template <bool INTER>
 __device__ void recon_block(const Ctx &c, Smem &sm, BlockInfo *gb) {
@@ -923,12 +962,11 @@ __device__ void recon_block(const Ctx &c, Smem &sm, BlockInfo *gb) {
       pred::inter_setup(&ip, ref + fp->offset[0], stride, fp->frame_w, fp->frame_h, x0, y0, w, h, b.mv_row, b.mv_col,
                         0, 0, packed);
       long long sse = 0;
+      predict_block(sm, ip, floor_log2(w), h, 0, px, rs);
       for (int k = tid; k < w * h; k += RT) {
         int i = k / w, j = k % w;
-        int v = pred::inter_pixel(&ip, i, j);
-        px[i * rs + j] = (uint8_t)v;
         if (i < vh && j < vw) {
-          int d = v - (int)sp[i * stride + j];
+          int d = (int)px[i * rs + j] - (int)sp[i * stride + j];
           sse += d * d;
         }
       }
@@ -961,13 +999,12 @@ __device__ void recon_block(const Ctx &c, Smem &sm, BlockInfo *gb) {
       if (comp)
         pred::inter_setup(&p1, ref1 + fp->offset[plane], stride, fp->frame_w, fp->frame_h, baseX, baseY, w, h,
                           b.mv1_row, b.mv1_col, sub, sub, b.interp_filter);
-      for (int k = tid; k < w * h; k += RT) {
-        int i = k / w, j = k % w;
-        int v = comp ? clip1(round2(pred::inter_raw(&p0, i, j) + pred::inter_raw(&p1, i, j), 5))
-                     : pred::inter_pixel(&p0, i, j);
-        d[i * rs + j] = (uint8_t)v;
+      if (comp) {
+        predict_block(sm, p0, floor_log2(w), h, 1, d, rs);
+        predict_block(sm, p1, floor_log2(w), h, 2, d, rs);
+      } else {
+        predict_block(sm, p0, floor_log2(w), h, 0, d, rs);
       }
-      __syncthreads();
     }
     if (fp->lossless) {
       code_plane<INTER>(c, sm, plane, TX_4X4);
