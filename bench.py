@@ -253,7 +253,7 @@ def roofline(kern, peaks):
     name = max(kern, key=kern.get)
     fb = 3133440  # padded 1080p frame bytes
     nsb = 510
-    alg = {  # compulsory bytes per launch of each stage (measurement section)
+    alg = {  # compulsory bytes per launch of each stage at 1080p: frames read or written once, tables once
         "motion_search": 3 * fb + 16 * 1920 * 1080 + nsb * 85 * 8,
         "analyze": 3 * fb + nsb * 85 * 13 * (8 + 108) // 13 + nsb * 64 * 108,
         "edge_types": 2 * nsb * 64 * 108,
