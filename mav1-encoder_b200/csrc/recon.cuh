@@ -197,8 +197,12 @@ __device__ void inv_col(Smem &sm, int j, int w, int ck, int fud, int flr, uint8_
 // dequantisation of 7.12.3), into sm.resid (stride 64).
 // With rec set, the column pass adds its output straight into the
 // reconstruction (flipped for FLIPADST types) instead of storing it.
-__device__ void inverse_2d(Smem &sm, const int32_t *q, int txSz, int txType, int dcQ, int acQ, uint8_t *rec = nullptr,
-                           int rs = 0, int x = 0, int y = 0) {
+// MAXL: the largest log2 length the instantiation handles; the sizes up to
+// 16 get their own inlined copy, so their register allocation does not
+// carry the 32- and 64-point kernels.
+template <int MAXL>
+__device__ __forceinline__ void inverse_2d_upto(Smem &sm, const int32_t *q, int txSz, int txType, int dcQ, int acQ,
+                                                uint8_t *rec, int rs, int x, int y) {
   int lw = T(Tx_Width_Log2)[txSz], lh = T(Tx_Height_Log2)[txSz];
   int w = 1 << lw, h = 1 << lh, th = imin(32, h);
   int rowShift = T(Transform_Row_Shift)[txSz], denom = tx::dq_denom(txSz);
@@ -209,8 +213,8 @@ __device__ void inverse_2d(Smem &sm, const int32_t *q, int txSz, int txType, int
       case 2: inv_row<2>(sm, q, i, th, dcQ, acQ, denom, rect, rk, rowShift); break;
       case 3: inv_row<3>(sm, q, i, th, dcQ, acQ, denom, rect, rk, rowShift); break;
       case 4: inv_row<4>(sm, q, i, th, dcQ, acQ, denom, rect, rk, rowShift); break;
-      case 5: inv_row<5>(sm, q, i, th, dcQ, acQ, denom, rect, rk, rowShift); break;
-      default: inv_row<6>(sm, q, i, th, dcQ, acQ, denom, rect, rk, rowShift); break;
+      case 5: if (MAXL >= 5) inv_row<5>(sm, q, i, th, dcQ, acQ, denom, rect, rk, rowShift); break;
+      default: if (MAXL >= 6) inv_row<6>(sm, q, i, th, dcQ, acQ, denom, rect, rk, rowShift); break;
     }
   }
   __syncthreads();
@@ -220,11 +224,28 @@ __device__ void inverse_2d(Smem &sm, const int32_t *q, int txSz, int txType, int
       case 2: inv_col<2>(sm, j, w, ck, fud, flr, rec, rs, x, y); break;
       case 3: inv_col<3>(sm, j, w, ck, fud, flr, rec, rs, x, y); break;
       case 4: inv_col<4>(sm, j, w, ck, fud, flr, rec, rs, x, y); break;
-      case 5: inv_col<5>(sm, j, w, ck, fud, flr, rec, rs, x, y); break;
-      default: inv_col<6>(sm, j, w, ck, fud, flr, rec, rs, x, y); break;
+      case 5: if (MAXL >= 5) inv_col<5>(sm, j, w, ck, fud, flr, rec, rs, x, y); break;
+      default: if (MAXL >= 6) inv_col<6>(sm, j, w, ck, fud, flr, rec, rs, x, y); break;
     }
   }
   __syncthreads();
+}
+
+__device__ __noinline__ void inverse_2d_large(Smem &sm, const int32_t *q, int txSz, int txType, int dcQ, int acQ,
+                                              uint8_t *rec, int rs, int x, int y) {
+  inverse_2d_upto<6>(sm, q, txSz, txType, dcQ, acQ, rec, rs, x, y);
+}
+
+// SMALL_INLINE: sizes up to 16 inlined (the intra workers, whose chains
+// wait on these latencies); otherwise every size through the out-of-line
+// copy (the inter kernel, where that keeps its register budget).
+template <bool SMALL_INLINE>
+__device__ __forceinline__ void inverse_2d(Smem &sm, const int32_t *q, int txSz, int txType, int dcQ, int acQ,
+                                           uint8_t *rec = nullptr, int rs = 0, int x = 0, int y = 0) {
+  if (SMALL_INLINE && T(Tx_Width_Log2)[txSz] <= 4 && T(Tx_Height_Log2)[txSz] <= 4)
+    inverse_2d_upto<4>(sm, q, txSz, txType, dcQ, acQ, rec, rs, x, y);
+  else
+    inverse_2d_large(sm, q, txSz, txType, dcQ, acQ, rec, rs, x, y);
 }
 
 // Forward matrix of a kind and length: lengths 4..16 from the CTA's shared
@@ -275,7 +296,8 @@ __device__ __forceinline__ int64_t fwd_col(const Smem &sm, const int32_t *Mv, in
 
 // Transform, quantise and reconstruct one transform block whose prediction
 // is in `rec` (code_tx_block, k_recon.h:60-173). Returns the eob.
-__device__ int code_tx(const Ctx &c, Smem &sm, const uint8_t *src, int stride, uint8_t *rec, int rs, int x, int y, int txSz,
+template <bool INTER>
+__device__ __forceinline__ int code_tx(const Ctx &c, Smem &sm, const uint8_t *src, int stride, uint8_t *rec, int rs, int x, int y, int txSz,
                        int plane, const int *cands, int numCands, int32_t *coefOut, int *outType, long long *outCost) {
   const FrameParams *fp = c.fp;
   int lw = T(Tx_Width_Log2)[txSz], lh = T(Tx_Height_Log2)[txSz];
@@ -397,7 +419,7 @@ __device__ int code_tx(const Ctx &c, Smem &sm, const uint8_t *src, int stride, u
       // only "has coefficients" matters here (the writer derives the eob)
       int nz = __syncthreads_or(myNz);
       for (int k = tid; k < tw * th; k += RT) coefOut[k] = sm.q[k];
-      if (nz) inverse_2d(sm, sm.q, txSz, t, dcQ, acQ, rec, rs, x, y);
+      if (nz) inverse_2d<!INTER>(sm, sm.q, txSz, t, dcQ, acQ, rec, rs, x, y);
       *outType = nz ? t : DCT_DCT;
       *outCost = 0;
       return nz;
@@ -406,7 +428,7 @@ __device__ int code_tx(const Ctx &c, Smem &sm, const uint8_t *src, int stride, u
     long long sse = 0;
     if (eob > 0) {
       // keep the residual-free path's SSE source intact: the inverse reuses resid
-      inverse_2d(sm, sm.q, txSz, t, dcQ, acQ);
+      inverse_2d<!INTER>(sm, sm.q, txSz, t, dcQ, acQ);
       for (int k = tid; k < h * w; k += RT) {
         int i = k >> lw, j = k & (w - 1);
         int yy = fud ? (h - 1 - i) : i, xx = flr ? (w - 1 - j) : j;
@@ -446,7 +468,7 @@ __device__ int code_tx(const Ctx &c, Smem &sm, const uint8_t *src, int stride, u
   for (int k = tid; k < tw * th; k += RT) coefOut[k] = qsrc[k];
   if (bestEob > 0) {
     int fud = tx::flip_ud(bestType), flr = tx::flip_lr(bestType);
-    if (numCands > 1) inverse_2d(sm, qsrc, txSz, bestType, dcQ, acQ);
+    if (numCands > 1) inverse_2d<!INTER>(sm, qsrc, txSz, bestType, dcQ, acQ);
     for (int k = tid; k < h * w; k += RT) {
       int i = k >> lw, j = k & (w - 1);
       int yy = fud ? (h - 1 - i) : i, xx = flr ? (w - 1 - j) : j;
@@ -865,7 +887,7 @@ __device__ long long code_plane(const Ctx &c, Smem &sm, int plane, int txSz) {
       }
       int t = DCT_DCT;
       long long cst = 0;
-      int eob = code_tx(c, sm, spx, stride, px, rs, startX, startY, txSz, plane, cands, numCands,
+      int eob = code_tx<INTER>(c, sm, spx, stride, px, rs, startX, startY, txSz, plane, cands, numCands,
                         c.coefs + b.coef_off[plane] + txIdx * T(Tx_Width)[txSz] * T(Tx_Height)[txSz], &t, &cst);
       total += cst;
       if (threadIdx.x == 0 && plane == 0) {
