@@ -48,6 +48,29 @@ __device__ __forceinline__ long long warp_sum64(long long v) {
   return v;
 }
 
+// The threads evaluating one candidate: a warp (rank = lane), or for the
+// 64x64 level a whole CTA (red: one shared word per warp). Sums are the
+// warp sums, then across the CTA's warps.
+struct Grp {
+  int rank, size;
+  long long *red;
+};
+__device__ __forceinline__ void gsync(const Grp &g) {
+  if (g.size == 32) __syncwarp();
+  else __syncthreads();
+}
+__device__ __forceinline__ long long gsum64(long long v, const Grp &g) {
+  v = warp_sum64(v);
+  if (g.size == 32) return v;
+  __syncthreads();
+  if ((g.rank & 31) == 0) g.red[g.rank >> 5] = v;
+  __syncthreads();
+  long long t = 0;
+  for (int k = 0; k < (g.size >> 5); k++) t += g.red[k];
+  return t;
+}
+__device__ __forceinline__ int gsum(int v, const Grp &g) { return (int)gsum64(v, g); }
+
 HD int mode_bits8(int mode) {
   if (mode == DC_PRED) return 12;
   if (mode == V_PRED || mode == H_PRED || mode == SMOOTH_PRED || mode == PAETH_PRED) return 26;
@@ -69,7 +92,7 @@ HD int eval_sub(const FrameParams *fp) { return (fp->turbo & T_ANA_USUB) != 0; }
 // block_satd_e of one plane predicted from one reference (k_analysis.h:113-119):
 // checkerboard units x2 when the analysis subsampling is on and bw >= 32.
 __device__ int inter_plane_satd(const FrameParams *fp, const uint8_t *src, const uint8_t *ref, int p, int bx, int by,
-                                int bw, int bh, int mvr, int mvc, int lane) {
+                                int bw, int bh, int mvr, int mvc, const Grp &g) {
   int sub = p > 0, stride = fp->stride[p];
   pred::Inter ip;
   pred::inter_setup(&ip, ref + fp->offset[p], stride, fp->frame_w, fp->frame_h, bx, by, bw, bh, mvr, mvc, sub, sub,
@@ -77,7 +100,7 @@ __device__ int inter_plane_satd(const FrameParams *fp, const uint8_t *src, const
   const uint8_t *sp = src + fp->offset[p] + by * stride + bx;
   int usub = eval_sub(fp) && bw >= 32 ? 2 : 1;
   int nux = bw >> 2, nu = nux * (bh >> 2), s = 0;
-  for (int u = lane; u < nu; u += 32) {
+  for (int u = g.rank; u < nu; u += g.size) {
     int ux = (u % nux) * 4, uy = (u / nux) * 4;
     if (usub > 1 && (((uy >> 2) + (ux >> 2)) & 1)) continue;
     int d[16];
@@ -85,13 +108,13 @@ __device__ int inter_plane_satd(const FrameParams *fp, const uint8_t *src, const
       for (int c = 0; c < 4; c++) d[r * 4 + c] = (int)sp[(uy + r) * stride + ux + c] - pred::inter_pixel(&ip, uy + r, ux + c);
     s += pred::satd4x4(d);
   }
-  return warp_sum(s) * usub;
+  return gsum(s, g) * usub;
 }
 
 // LAST, second reference and compound-average SATDs of all planes with each
 // plane's two predictions computed once (inter3_satd, k_analysis.h:202-235).
 __device__ void inter3(const FrameParams *fp, const uint8_t *src, const uint8_t *ref, const uint8_t *ref2, int x, int y,
-                       int w, int h, int mvr, int mvc, int mvr2, int mvc2, long long *s, int lane) {
+                       int w, int h, int mvr, int mvc, int mvr2, int mvc2, long long *s, const Grp &g) {
   long long a0 = 0, a1 = 0, a2 = 0;
   for (int p = 0; p < 3; p++) {
     int sub = p > 0;
@@ -105,7 +128,7 @@ __device__ void inter3(const FrameParams *fp, const uint8_t *src, const uint8_t 
     int usub = eval_sub(fp) && bw >= 32 ? 2 : 1;
     int nux = bw >> 2, nu = nux * (bh >> 2);
     int l0 = 0, l1 = 0, l2 = 0;
-    for (int u = lane; u < nu; u += 32) {
+    for (int u = g.rank; u < nu; u += g.size) {
       int ux = (u % nux) * 4, uy = (u / nux) * 4;
       if (usub > 1 && (((uy >> 2) + (ux >> 2)) & 1)) continue;
       int d0[16], d1[16], d2[16];
@@ -125,9 +148,9 @@ __device__ void inter3(const FrameParams *fp, const uint8_t *src, const uint8_t 
     a1 += (long long)l1 * usub;
     a2 += (long long)l2 * usub;
   }
-  s[0] = warp_sum64(a0);
-  s[1] = warp_sum64(a1);
-  s[2] = warp_sum64(a2);
+  s[0] = gsum64(a0, g);
+  s[1] = gsum64(a1, g);
+  s[2] = gsum64(a2, g);
 }
 
 // ---- intra SATDs ----------------------------------------------------------------
@@ -155,27 +178,27 @@ __device__ __forceinline__ pred::IntraArgs ana_args(const FrameParams *fp, int p
 
 // Edge arrays of one plane block (mode independent without the edge filter).
 __device__ void build_edges(const FrameParams *fp, const uint8_t *plane, int stride, int planeIdx, int x, int y, int lw,
-                            int lh, int *above, int *left, int lane) {
+                            int lh, int *above, int *left, const Grp &g) {
   pred::IntraArgs a = ana_args(fp, planeIdx, x, y, lw, lh, DC_PRED, 0);
   int n = (1 << lw) + (1 << lh);
-  for (int i = lane; i < n; i += 32) {
+  for (int i = g.rank; i < n; i += g.size) {
     above[i] = pred::above_sample(plane, stride, x, y, a, i);
     left[i] = pred::left_sample(plane, stride, x, y, a, i);
   }
-  if (lane == 0) above[-1] = left[-1] = pred::corner_sample(plane, stride, x, y, a);
-  __syncwarp();
+  if (g.rank == 0) above[-1] = left[-1] = pred::corner_sample(plane, stride, x, y, a);
+  gsync(g);
 }
 
 // block_satd_s of the intra prediction `mode` (+delta) against the source.
 __device__ int intra_mode_satd(const FrameParams *fp, const uint8_t *plane, int stride, int planeIdx, int x, int y,
-                               int lw, int lh, int mode, int delta, const int *above, const int *left, int lane) {
+                               int lw, int lh, int mode, int delta, const int *above, const int *left, const Grp &g) {
   pred::IntraArgs a = ana_args(fp, planeIdx, x, y, lw, lh, mode, delta);
   pred::IntraState st;
   pred::intra_state(a, &st);
   int dc = mode == DC_PRED ? pred::intra_dc(a, above, left) : 0;
   int w = 1 << lw, h = 1 << lh, nux = w >> 2, nu = nux * (h >> 2), s = 0;
   const uint8_t *sp = plane + y * stride + x;
-  for (int u = lane; u < nu; u += 32) {
+  for (int u = g.rank; u < nu; u += g.size) {
     int ux = (u % nux) * 4, uy = (u / nux) * 4;
     int d[16];
     for (int r = 0; r < 4; r++)
@@ -185,14 +208,14 @@ __device__ int intra_mode_satd(const FrameParams *fp, const uint8_t *plane, int 
       }
     s += pred::satd4x4(d);
   }
-  return warp_sum(s);
+  return gsum(s, g);
 }
 
 // CfL SATD of one chroma plane from source luma: DC prediction, the first
 // minimum-SSE alpha in [-16, 16], then the SATD of the CfL prediction
 // (k_analysis.h:349-365 with cfl_best_alpha / cfl_predict, k_intra.h:252-313).
 __device__ int cfl_plane_satd(const FrameParams *fp, const uint8_t *src, int p, int cx, int cy, int clw, int clh,
-                              int maxLumaW, int maxLumaH, const int *above, const int *left, int lane) {
+                              int maxLumaW, int maxLumaH, const int *above, const int *left, const Grp &g) {
   pred::IntraArgs a = ana_args(fp, p, cx, cy, clw, clh, DC_PRED, 0);
   int dc = pred::intra_dc(a, above, left);
   int cw = 1 << clw, ch = 1 << clh, n = cw * ch;
@@ -200,11 +223,11 @@ __device__ int cfl_plane_satd(const FrameParams *fp, const uint8_t *src, int p, 
   int ls = fp->stride[0], stride = fp->stride[p];
   const uint8_t *sp = src + fp->offset[p] + cy * stride + cx;
   int sum = 0;
-  for (int k = lane; k < n; k += 32) sum += pred::cfl_luma(luma, ls, cx, cy, maxLumaW, maxLumaH, k / cw, k % cw);
-  int avg = round2(warp_sum(sum), clw + clh);
+  for (int k = g.rank; k < n; k += g.size) sum += pred::cfl_luma(luma, ls, cx, cy, maxLumaW, maxLumaH, k / cw, k % cw);
+  int avg = round2(gsum(sum, g), clw + clh);
   int sse[33];
   for (int al = 0; al < 33; al++) sse[al] = 0;
-  for (int k = lane; k < n; k += 32) {
+  for (int k = g.rank; k < n; k += g.size) {
     int i = k / cw, j = k % cw;
     int v = pred::cfl_luma(luma, ls, cx, cy, maxLumaW, maxLumaH, i, j) - avg;
     int s0 = sp[i * stride + j];
@@ -216,14 +239,14 @@ __device__ int cfl_plane_satd(const FrameParams *fp, const uint8_t *src, int p, 
   int bestA = 0;
   long long best = -1;
   for (int al = 0; al < 33; al++) {
-    long long t = warp_sum64(sse[al]);
+    long long t = gsum64(sse[al], g);
     if (best < 0 || t < best) {
       best = t;
       bestA = al - 16;
     }
   }
   int nux = cw >> 2, nu = nux * (ch >> 2), s = 0;
-  for (int u = lane; u < nu; u += 32) {
+  for (int u = g.rank; u < nu; u += g.size) {
     int ux = (u % nux) * 4, uy = (u / nux) * 4;
     int d[16];
     for (int r = 0; r < 4; r++)
@@ -233,12 +256,12 @@ __device__ int cfl_plane_satd(const FrameParams *fp, const uint8_t *src, int p, 
       }
     s += pred::satd4x4(d);
   }
-  return warp_sum(s);
+  return gsum(s, g);
 }
 
 // ---- eval_block (k_analysis.h:241-404) --------------------------------------------
 __device__ long long eval_block(const Ctx &c, int mvNode, int miRow, int miCol, int bsize, BlockInfo *out,
-                                WarpMem &wm, int lane) {
+                                WarpMem &wm, const Grp &g) {
   const FrameParams *fp = c.fp;
   int lw = T(Mi_Width_Log2)[bsize] + 2, lh = T(Mi_Height_Log2)[bsize] + 2;
   int w = 1 << lw, h = 1 << lh;
@@ -253,7 +276,7 @@ __device__ long long eval_block(const Ctx &c, int mvNode, int miRow, int miCol, 
     const int32_t *m1 = c.mvg + (sbIdx * NUM_NODES + mvNode) * 2;
     int lr = m0[0], lc = m0[1], gr = m1[0], gc = m1[1];
     long long s[3];
-    inter3(fp, c.src, c.ref, c.gold, x, y, w, h, lr, lc, gr, gc, s, lane);
+    inter3(fp, c.src, c.ref, c.gold, x, y, w, h, lr, lc, gr, gc, s, g);
     interCost = s[0] + (long long)lam * (4 + mv_bits8(lr, lc)) / 8;
     mvr = lr;
     mvc = lc;
@@ -279,8 +302,8 @@ __device__ long long eval_block(const Ctx &c, int mvNode, int miRow, int miCol, 
       const int32_t *mp = (r ? c.mvg : c.mv) + (sbIdx * NUM_NODES + mvNode) * 2;
       const uint8_t *rp = r ? c.gold : c.ref;
       int qr = mp[0], qc = mp[1];
-      long long cost = inter_plane_satd(fp, c.src, rp, 0, x, y, w, h, qr, qc, lane);
-      for (int p = 1; p < 3; p++) cost += inter_plane_satd(fp, c.src, rp, p, cx, cy, w >> 1, h >> 1, qr, qc, lane);
+      long long cost = inter_plane_satd(fp, c.src, rp, 0, x, y, w, h, qr, qc, g);
+      for (int p = 1; p < 3; p++) cost += inter_plane_satd(fp, c.src, rp, p, cx, cy, w >> 1, h >> 1, qr, qc, g);
       cost += (long long)lam * (4 + mv_bits8(qr, qc)) / 8;
       if (r == 0) {
         interCost = cost;
@@ -303,10 +326,10 @@ __device__ long long eval_block(const Ctx &c, int mvNode, int miRow, int miCol, 
   int skipIntra = interCost >= 0 && (fp->leaf || (fp->fast && interCost * 16 < (long long)w * h * lam * 16));
   int *ya = wm.edge[0][0] + EDGE_OFF, *yl = wm.edge[0][1] + EDGE_OFF;
   if (!skipIntra) {
-    build_edges(fp, c.src + fp->offset[0], fp->stride[0], 0, x, y, lw, lh, ya, yl, lane);
+    build_edges(fp, c.src + fp->offset[0], fp->stride[0], 0, x, y, lw, lh, ya, yl, g);
     for (int mode = DC_PRED; mode <= PAETH_PRED; mode++) {
       if (turbo_mode_off(fp, mode)) continue;
-      long long cst = intra_mode_satd(fp, c.src + fp->offset[0], fp->stride[0], 0, x, y, lw, lh, mode, 0, ya, yl, lane) +
+      long long cst = intra_mode_satd(fp, c.src + fp->offset[0], fp->stride[0], 0, x, y, lw, lh, mode, 0, ya, yl, g) +
                       (long long)lam * mode_bits8(mode) / 8;
       if (best < 0 || cst < best) {
         best = cst;
@@ -319,7 +342,7 @@ __device__ long long eval_block(const Ctx &c, int mvNode, int miRow, int miCol, 
     int base = bestMode;
     for (int d = -MAX_ANGLE_DELTA; d <= MAX_ANGLE_DELTA; d++) {
       if (d == 0) continue;
-      long long cst = intra_mode_satd(fp, c.src + fp->offset[0], fp->stride[0], 0, x, y, lw, lh, base, d, ya, yl, lane) +
+      long long cst = intra_mode_satd(fp, c.src + fp->offset[0], fp->stride[0], 0, x, y, lw, lh, base, d, ya, yl, g) +
                       (long long)lam * (mode_bits8(base) + 16) / 8;
       if (cst < best) {
         best = cst;
@@ -333,7 +356,7 @@ __device__ long long eval_block(const Ctx &c, int mvNode, int miRow, int miCol, 
   if (!skipUv) {
     for (int p = 1; p < 3; p++)
       build_edges(fp, c.src + fp->offset[p], fp->stride[p], p, cx, cy, clw, clh, wm.edge[p][0] + EDGE_OFF,
-                  wm.edge[p][1] + EDGE_OFF, lane);
+                  wm.edge[p][1] + EDGE_OFF, g);
     for (int m = DC_PRED; m <= PAETH_PRED; m++) {
       if (intra_is_directional(m) && m != V_PRED && m != H_PRED && m != bestMode) continue;
       if (turbo_mode_off(fp, m)) continue;
@@ -341,7 +364,7 @@ __device__ long long eval_block(const Ctx &c, int mvNode, int miRow, int miCol, 
       long long cst = 0;
       for (int p = 1; p < 3; p++)
         cst += intra_mode_satd(fp, c.src + fp->offset[p], fp->stride[p], p, cx, cy, clw, clh, m, delta,
-                               wm.edge[p][0] + EDGE_OFF, wm.edge[p][1] + EDGE_OFF, lane);
+                               wm.edge[p][0] + EDGE_OFF, wm.edge[p][1] + EDGE_OFF, g);
       cst += (long long)lam * (m == DC_PRED ? 8 : 24) / 8;
       if (bestUv < 0 || cst < bestUv) {
         bestUv = cst;
@@ -352,7 +375,7 @@ __device__ long long eval_block(const Ctx &c, int mvNode, int miRow, int miCol, 
       long long cst = (long long)lam * 40 / 8;
       for (int p = 1; p < 3; p++)
         cst += cfl_plane_satd(fp, c.src, p, cx, cy, clw, clh, x + w, y + h, wm.edge[p][0] + EDGE_OFF,
-                              wm.edge[p][1] + EDGE_OFF, lane);
+                              wm.edge[p][1] + EDGE_OFF, g);
       if (cst < bestUv) {
         bestUv = cst;
         bestUvMode = UV_CFL_PRED;
@@ -497,17 +520,23 @@ __device__ int depth_pruned(const FrameParams *fp, const int64_t *costs, int sbI
   return 0;
 }
 
-// Pass 1 of one level: warp per item (superblock, node, slot), items in the
-// reference's order sb-major (k_analysis.h:656-679).
-__global__ void __launch_bounds__(128) k_analyze_level(Ctx c, int level, int slots) {
+// Pass 1 of one level: items (superblock, node, slot) in the reference's
+// order sb-major (k_analysis.h:656-679). A warp per item, or with
+// whole_cta the CTA's four warps on one item (the 64x64 level, whose few
+// large items would otherwise leave most SMs idle).
+#define ANA_THREADS 128
+__global__ void __launch_bounds__(ANA_THREADS) k_analyze_level(Ctx c, int level, int slots, int whole_cta) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   WarpMem *wmem = (WarpMem *)smem_raw;
+  long long *red = (long long *)(wmem + ANA_THREADS / 32);
   const FrameParams *fp = c.fp;
   int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   int n = 1 << level, per = n * n * slots;
-  int g = blockIdx.x * (blockDim.x >> 5) + warp;
-  if (g >= fp->sb_cols * fp->sb_rows * per) return;
-  int sbIdx = g / per, rem = g % per, i = rem / slots, slot = rem % slots;
+  int item = whole_cta ? (int)blockIdx.x : (int)blockIdx.x * (ANA_THREADS / 32) + warp;
+  Grp grp = whole_cta ? Grp{(int)threadIdx.x, ANA_THREADS, red} : Grp{lane, 32, nullptr};
+  WarpMem &wm = wmem[whole_cta ? 0 : warp];
+  if (item >= fp->sb_cols * fp->sb_rows * per) return;
+  int sbIdx = item / per, rem = item % per, i = rem / slots, slot = rem % slots;
   int sbRow = sbIdx / fp->sb_cols, sbCol = sbIdx % fp->sb_cols;
   int size4 = 16 >> level, halfSz = size4 >> 1;
   int node = node_base(level) + i;
@@ -523,14 +552,14 @@ __global__ void __launch_bounds__(128) k_analyze_level(Ctx c, int level, int slo
     skip = !part_allowed(fp, level, p, hasRows, hasCols) || k >= part_count(fp, p, r, cc, halfSz);
   }
   if (skip) {
-    if (lane == 0) c.costs[idx] = -1;
+    if (grp.rank == 0) c.costs[idx] = -1;
     return;
   }
   int dr, dc;
   int bs = part_block(p, level_bsize(level), k, halfSz, &dr, &dc);
   BlockInfo b;
-  long long cost = eval_block(c, node, r + dr, cc + dc, bs, &b, wmem[warp], lane);
-  if (lane == 0) {
+  long long cost = eval_block(c, node, r + dr, cc + dc, bs, &b, wm, grp);
+  if (grp.rank == 0) {
     c.costs[idx] = cost;
     c.infos[idx] = b;
   }

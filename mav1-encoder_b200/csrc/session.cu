@@ -23,6 +23,10 @@
 #include "filters.cuh"
 #include "stream.cuh"
 
+// dynamic shared memory of the analysis pass-1 kernel: a WarpMem per warp
+// and one reduction word per warp
+#define ANA_SMEM (ANA_THREADS / 32 * sizeof(ana::WarpMem) + ANA_THREADS / 32 * sizeof(long long))
+
 namespace {
 
 struct Geometry {
@@ -311,8 +315,7 @@ extern "C" int mav1cu_session_create(int width, int height, int max_cdef_presets
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, rec::k_recon_blocks, rec::INTRA_THREADS, sizeof(rec::Smem));
     s->resident_recon = imax(1, sms * imax(1, per));
   }
-  cudaFuncSetAttribute(ana::k_analyze_level, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)(4 * sizeof(ana::WarpMem)));
+  cudaFuncSetAttribute(ana::k_analyze_level, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ANA_SMEM);
   *out = s;
   return MAV1CU_OK;
 }
@@ -466,7 +469,9 @@ extern "C" int mav1cu_analyze(mav1cu_session *s) {
   for (int level = 0; level < 4; level++) {
     int slots = ana::level_slots(&s->fp, level);
     long long items = (long long)s->g.num_sbs * (1 << (2 * level)) * slots;
-    ana::k_analyze_level<<<(unsigned)((items + 3) / 4), 128, 4 * sizeof(ana::WarpMem), s->stream>>>(c, level, slots);
+    int whole = level == 0;  // the 64x64 candidates: one CTA each
+    unsigned grid = (unsigned)(whole ? items : (items + ANA_THREADS / 32 - 1) / (ANA_THREADS / 32));
+    ana::k_analyze_level<<<grid, ANA_THREADS, ANA_SMEM, s->stream>>>(c, level, slots, whole);
     if (after_launch(s, "analysis pass 1")) return s->err;
   }
   ana::k_analyze_table<<<(s->g.num_sbs + TABLE_WARPS - 1) / TABLE_WARPS, 32 * TABLE_WARPS, 0, s->stream>>>(c);
