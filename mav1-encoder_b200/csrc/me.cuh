@@ -259,47 +259,61 @@ __device__ __forceinline__ void sub_neighbour(const FrameParams *fp, int j, int 
   *dc = (k == 0 || k == 3 || k == 5) ? -step : ((k == 1 || k == 6) ? 0 : step);
 }
 
+// The threads searching one node: a warp, or for the 64x64 level the CTA.
+struct MeGrp {
+  int rank, size;
+  __device__ __forceinline__ void sync() const {
+    if (size == 32) __syncwarp();
+    else __syncthreads();
+  }
+};
+
 // Sub-pel costs of ncand candidates (mvr[c], mvc[c]) into cost[c] (shared,
-// warp-private), every (candidate, unit) pair spread over the lanes.
+// private to the group), every (candidate, unit) pair spread over the group.
 __device__ void subpel_costs(const Frame &f, const Node &m, const int *cr, const int *cc, int ncand, int *cost,
-                             int lane) {
+                             const MeGrp &g) {
   const FrameParams *fp = f.fp;
   int hp = (fp->turbo & T_ME_HPEL) != 0;
   int nu = (m.w >> 2) * (m.w >> 2);
   int st = hp && (fp->turbo & T_ME_USUB) && m.w >= 32 ? 2 : 1;
   int nus = (nu + st - 1) / st;
-  if (lane < ncand) cost[lane] = 0;
-  __syncwarp();
-  for (int p = lane; p < ncand * nus; p += 32) {
+  if (g.rank < ncand) cost[g.rank] = 0;
+  g.sync();
+  for (int p = g.rank; p < ncand * nus; p += g.size) {
     int c = p / nus, u = (p % nus) * st;
     int s = hp ? unit_satd_hp(f, m, cr[c], cc[c], u) : unit_satd_pred(f, m, cr[c], cc[c], u);
     atomicAdd(&cost[c], s);
   }
-  __syncwarp();
-  if (lane < ncand) cost[lane] *= st;
-  __syncwarp();
+  g.sync();
+  if (g.rank < ncand) cost[g.rank] *= st;
+  g.sync();
 }
 
-// One search level: warp per (node, reference); blockIdx.y selects the reference.
-__global__ void __launch_bounds__(128) k_me_level(Frame f0, Frame f1, int level) {
+// One search level: warp per (node, reference), or with whole_cta the
+// CTA's four warps per node (the 64x64 level: few, large nodes);
+// blockIdx.y selects the reference.
+__global__ void __launch_bounds__(128) k_me_level(Frame f0, Frame f1, int level, int whole_cta) {
   __shared__ int s_cost[4][16];
   __shared__ int s_r[4][16], s_c[4][16];
+  __shared__ unsigned long long s_best[4];
   const Frame &f = blockIdx.y ? f1 : f0;
   const FrameParams *fp = f.fp;
   int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  MeGrp grp = whole_cta ? MeGrp{(int)threadIdx.x, 128} : MeGrp{lane, 32};
+  int slotw = whole_cta ? 0 : warp;
   int nn = 1 << (2 * level);
-  int g = blockIdx.x * 4 + warp;
+  int g = whole_cta ? (int)blockIdx.x : (int)blockIdx.x * 4 + warp;
   if (g >= fp->sb_cols * fp->sb_rows * nn) return;
   int sb = g / nn, i = g % nn;
   Node m = make_node(fp, sb, level, i, f.mv);
   if (f.isGold && level == 3 && (fp->turbo & T_ME_G3COPY) && fp->leaf && !fp->frame_is_intra) m.copy = 1;
   int32_t *out = f.mv + (sb * NUM_NODES + node_base(level) + i) * 2;
   if (!m.valid) {
-    if (lane == 0) out[0] = out[1] = 0;
+    if (grp.rank == 0) out[0] = out[1] = 0;
     return;
   }
   if (m.copy) {
-    if (lane == 0) {
+    if (grp.rank == 0) {
       out[0] = m.pr;
       out[1] = m.pc;
     }
@@ -309,44 +323,50 @@ __global__ void __launch_bounds__(128) k_me_level(Frame f0, Frame f1, int level)
   for (int stage = 0; stage < m.stages; stage++) {
     if (stage > 0) refine_stage(fp, &m, by, bx, stage);
     unsigned long long best = ~0ull;
-    for (int k = lane; k < m.count; k += 32) {
+    for (int k = grp.rank; k < m.count; k += grp.size) {
       int dy, dx;
       candidate(m, k, &dy, &dx);
       unsigned long long key = ((unsigned long long)(unsigned)full_cost(f, m, dy, dx) << 32) | (unsigned)k;
       best = key < best ? key : best;
     }
     best = warp_min_u64(best);
+    if (whole_cta) {
+      __syncthreads();
+      if (lane == 0) s_best[warp] = best;
+      __syncthreads();
+      for (int w = 0; w < 4; w++) best = s_best[w] < best ? s_best[w] : best;
+    }
     candidate(m, (int)(best & 0xffffffffu), &by, &bx);
   }
   if (level > 0 && (m.copy || ((fp->turbo & T_ME_KEEP) && by == m.cy && bx == m.cx))) {
-    if (lane == 0) {
+    if (grp.rank == 0) {
       out[0] = m.pr;
       out[1] = m.pc;
     }
     return;
   }
   // sub-pel refinement (k_me.h:262-281)
-  int *cost = s_cost[warp], *cr = s_r[warp], *cc = s_c[warp];
+  int *cost = s_cost[slotw], *cr = s_r[slotw], *cc = s_c[slotw];
   int mvr = m.stages ? by * 8 : m.pr, mvc = m.stages ? bx * 8 : m.pc;
-  if (lane == 0) {
+  if (grp.rank == 0) {
     cr[0] = mvr;
     cc[0] = mvc;
   }
-  __syncwarp();
-  subpel_costs(f, m, cr, cc, 1, cost, lane);
+  grp.sync();
+  subpel_costs(f, m, cr, cc, 1, cost, grp);
   int bestS = cost[0];
   int minStep = m.w >= 32 && (fp->turbo & T_ME_HALF01) ? 4 : 2;
   int nb = (fp->turbo & T_ME_CROSS) ? 4 : 8;
   for (int step = 4; step >= minStep; step >>= 1) {
-    __syncwarp();
-    if (lane < nb) {
+    grp.sync();
+    if (grp.rank < nb) {
       int dr, dc;
-      sub_neighbour(fp, lane, step, &dr, &dc);
-      cr[lane] = mvr + dr;
-      cc[lane] = mvc + dc;
+      sub_neighbour(fp, grp.rank, step, &dr, &dc);
+      cr[grp.rank] = mvr + dr;
+      cc[grp.rank] = mvc + dc;
     }
-    __syncwarp();
-    subpel_costs(f, m, cr, cc, nb, cost, lane);
+    grp.sync();
+    subpel_costs(f, m, cr, cc, nb, cost, grp);
     // running strict minimum over the neighbours in order == first minimum
     int bk = -1, bc = bestS;
     for (int k = 0; k < nb; k++)
@@ -360,7 +380,7 @@ __global__ void __launch_bounds__(128) k_me_level(Frame f0, Frame f1, int level)
       mvc = cc[bk];
     }
   }
-  if (lane == 0) {
+  if (grp.rank == 0) {
     out[0] = mvr;
     out[1] = mvc;
   }

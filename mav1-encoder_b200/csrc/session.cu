@@ -441,8 +441,9 @@ extern "C" int mav1cu_motion_search(mav1cu_session *s) {
   }
   for (int level = 0; level < 4; level++) {
     int nodes = s->g.num_sbs << (2 * level);
-    dim3 grid((nodes + 3) / 4, nref);
-    me::k_me_level<<<grid, 128, 0, s->stream>>>(f[0], f[1], level);
+    int whole = level == 0;  // the 64x64 nodes: one CTA each
+    dim3 grid(whole ? nodes : (nodes + 3) / 4, nref);
+    me::k_me_level<<<grid, 128, 0, s->stream>>>(f[0], f[1], level, whole);
     if (after_launch(s, "motion search")) return s->err;
   }
   return MAV1CU_OK;
