@@ -394,7 +394,10 @@ extern "C" int mav1cu_set_params(mav1cu_session *s, const mav1cu_frame_params *f
   s->fp = *fp;
   s->have_params = 1;
   if (s->wave_tile_w != fp->tile_w_sb && build_waves(s, fp->tile_w_sb)) return s->err;
-  return mav1cu_upload(s, MAV1CU_BUF_PARAMS, fp, sizeof(FrameParams));
+  // by value through a launch: asynchronous for any caller memory (a copy
+  // from pageable memory may wait for the stream's earlier work)
+  drv::k_store_params<<<1, 128, 0, s->stream>>>(*fp, (FrameParams *)s->buf[MAV1CU_BUF_PARAMS]);
+  return after_launch(s, "frame parameters");
 }
 
 static int need_params(mav1cu_session *s) {

@@ -278,6 +278,13 @@ static void frame_params(const Norm &n, const mav1cu_frame_job &j, FrameParams *
 
 // Packed I420 -> padded planes with right / bottom edge replication
 // (load_source, encoder.c:297-310).
+// Stores frame parameters passed by value (the launch copies them).
+__global__ void k_store_params(FrameParams fp, FrameParams *dst) {
+  const int *a = (const int *)&fp;
+  int *d = (int *)dst;
+  for (int k = threadIdx.x; k < (int)(sizeof(FrameParams) / 4); k += blockDim.x) d[k] = a[k];
+}
+
 __global__ void k_load_source(const uint8_t *i420, uint8_t *dst, int w, int h, int sbCols, int sbRows) {
   int p = blockIdx.z;
   int pw = p ? (w + 1) >> 1 : w, ph = p ? (h + 1) >> 1 : h;
