@@ -65,6 +65,11 @@ struct Ctx {
   int *status;          // [0] error code, [1] abort
   const int *blk_at;    // per 4x4 luma unit of the frame: index of the block covering it
   int *done;            // per block index: 1 once its luma samples are written; then the same for chroma
+  // the intra blocks' ready queue: unfinished luma dependencies per block,
+  // successor lists (blocks whose luma edges read this block's luma), and
+  // the queue of blocks whose luma dependencies are all complete
+  int *dep_count, *succ_count, *succ;
+  int *queue, *qvalid, *qtail;
 };
 
 #define TILE_OFF 4     // tile column of the block's first sample (word aligned; the left column at 3)
@@ -533,12 +538,60 @@ __device__ int cfl_alpha(Smem &sm, const uint8_t *luma, int ls, int startX, int 
 
 // The clear-flags value of a unit outside the superblock (superblock-relative
 // units of the plane, -1..n): clear_block_decoded_flags (k_recon.h:402-414).
-__device__ __forceinline__ int decoded_outside(const FrameParams *fp, const Smem &sm, int sub, int y, int x) {
+__device__ __forceinline__ int decoded_outside(const FrameParams *fp, int r0, int c0, int sub, int y, int x) {
   int n = 16 >> sub;
   if (y == n && x == -1) return 0;
-  if (y < 0) return x < ((tile_col_end(fp, sm.c0) - sm.c0) >> sub);
-  if (x < 0) return y < ((fp->mi_rows - sm.r0) >> sub);
+  if (y < 0) return x < ((tile_col_end(fp, c0) - c0) >> sub);
+  if (x < 0) return y < ((fp->mi_rows - r0) >> sub);
   return 0;
+}
+
+// BlockDecoded of the above-right (k = 0) or below-left (k = 1) corner unit of
+// plane p of block b (index me, superblock origin r0, c0) from the frame's
+// unit map: the clear-flags value outside the superblock, else whether the
+// block covering it precedes this one.
+__device__ __forceinline__ int corner_decoded(const FrameParams *fp, const int *blkAt, const BlockInfo &b, int me,
+                                              int r0, int c0, int p, int k) {
+  int sub = p > 0, n = 16 >> sub;
+  int top = (b.mi_row & 15) >> sub, left = (b.mi_col & 15) >> sub;
+  int y = k ? top + (block_h(b.bsize) >> (2 + sub)) : top - 1;
+  int x = k ? left - 1 : left + (block_w(b.bsize) >> (2 + sub));
+  if (y < 0 || x < 0 || y >= n || x >= n) return decoded_outside(fp, r0, c0, sub, y, x);
+  int r = r0 + (y << sub), col = c0 + (x << sub);
+  if (r >= fp->mi_rows || col >= fp->mi_cols) return 0;
+  int blk = blkAt[r * fp->mi_cols + col];
+  return blk >= 0 && blk < me;
+}
+
+// The edge samples plane p of block b can read (see stage_edges): row ay
+// from ax0 to ax1 and column x0 - 1 from ly0 to ly1 (empty runs: end <
+// start), and the 4x4 luma units under them as two runs (ur, uc, urow, un).
+struct EdgeRuns {
+  int ay, ax0, ax1, ly0, ly1;
+  int ur[2], uc[2], urow[2], un[2];
+};
+__device__ __forceinline__ EdgeRuns edge_runs(const FrameParams *fp, const BlockInfo &b, int p, int ar, int bl) {
+  EdgeRuns e;
+  int bs = b.bsize, sub = p > 0, w = block_w(bs) >> sub, h = block_h(bs) >> sub;
+  int availU = b.mi_row > 0, availL = b.mi_col > tile_col_start(fp, b.mi_col);
+  int x0 = (b.mi_col >> sub) * 4, y0 = (b.mi_row >> sub) * 4;
+  int txSz = fp->lossless ? TX_4X4 : sub ? uv_tx_size(bs, 1, 1) : T(Max_Tx_Size_Rect)[bs];
+  int ext = imin(T(Tx_Width)[txSz], T(Tx_Height)[txSz]);
+  int maxX = ((fp->mi_cols * 4) >> sub) - 1, maxY = ((fp->mi_rows * 4) >> sub) - 1;
+  e.ay = y0 - 1;
+  e.ax0 = x0 - availL;
+  e.ax1 = availU ? imin(maxX, x0 + w - 1 + (ar ? ext : 0)) : e.ax0 - 1;
+  e.ly0 = y0 - availU;
+  e.ly1 = availL ? imin(maxY, y0 + h - 1 + (bl ? ext : 0)) : e.ly0 - 1;
+  e.ur[0] = (e.ay << sub) >> 2;
+  e.uc[0] = (e.ax0 << sub) >> 2;
+  e.urow[0] = 1;
+  e.un[0] = e.ax1 >= e.ax0 ? ((e.ax1 << sub) >> 2) - e.uc[0] + 1 : 0;
+  e.ur[1] = (e.ly0 << sub) >> 2;
+  e.uc[1] = ((x0 - 1) << sub) >> 2;
+  e.urow[1] = 0;
+  e.un[1] = e.ly1 >= e.ly0 ? ((e.ly1 << sub) >> 2) - e.ur[1] + 1 : 0;
+  return e;
 }
 
 // BlockDecoded[plane][y][x] (superblock-relative units of the plane, -1..n)
@@ -556,7 +609,7 @@ __device__ __forceinline__ int decoded_outside(const FrameParams *fp, const Smem
 __device__ int decoded(const Ctx &c, const Smem &sm, int plane, int y, int x, int own) {
   const FrameParams *fp = c.fp;
   int sub = plane > 0, n = 16 >> sub;
-  if (y < 0 || x < 0 || y >= n || x >= n) return decoded_outside(fp, sm, sub, y, x);
+  if (y < 0 || x < 0 || y >= n || x >= n) return decoded_outside(fp, sm.r0, sm.c0, sub, y, x);
   if (sm.r0 + (y << sub) >= fp->mi_rows || sm.c0 + (x << sub) >= fp->mi_cols) return 0;
   const BlockInfo &b = sm.blk;
   int top = (b.mi_row & 15) >> sub, left = (b.mi_col & 15) >> sub;
@@ -696,7 +749,7 @@ __device__ void stage_begin(const Ctx &c, Smem &sm) {
     int y = k ? top + (h >> 2) : top - 1, x = k ? left - 1 : left + (w >> 2);
     int v;
     if (y < 0 || x < 0 || y >= n || x >= n) {
-      v = decoded_outside(fp, sm, sub, y, x);
+      v = decoded_outside(fp, sm.r0, sm.c0, sub, y, x);
     } else {
       int blk = sm.cornerBlk[tid];
       v = blk >= 0 && blk < sm.me;  // -1: beyond the frame
@@ -719,32 +772,27 @@ __device__ void stage_begin(const Ctx &c, Smem &sm) {
 __device__ void stage_edges(const Ctx &c, Smem &sm, int group) {
   const FrameParams *fp = c.fp;
   const BlockInfo &b = sm.blk;
-  int bs = b.bsize, p0 = group ? 1 : 0, np = group ? 2 : 1;
-  int availU = b.mi_row > 0, availL = b.mi_col > tile_col_start(fp, b.mi_col);
+  int p0 = group ? 1 : 0, np = group ? 2 : 1;
   int ay[2], ax0[2], ax1[2], ly0[2], ly1[2];
   int ur[6] = {0}, uc[6] = {0}, urow[6] = {0}, un[6] = {0};  // the 4x4 luma units under the edge samples
   for (int q = 0; q < np; q++) {
-    int p = p0 + q, sub = p > 0, w = block_w(bs) >> sub, h = block_h(bs) >> sub;
-    int x0 = (b.mi_col >> sub) * 4, y0 = (b.mi_row >> sub) * 4;
-    int txSz = fp->lossless ? TX_4X4 : sub ? uv_tx_size(bs, 1, 1) : T(Max_Tx_Size_Rect)[bs];
-    int ext = imin(T(Tx_Width)[txSz], T(Tx_Height)[txSz]);
-    int ar = sm.cornerAR[p], bl = sm.cornerBL[p];
-    int maxX = ((fp->mi_cols * 4) >> sub) - 1, maxY = ((fp->mi_rows * 4) >> sub) - 1;
-    ay[q] = y0 - 1;
-    ax0[q] = x0 - availL;
-    ax1[q] = availU ? imin(maxX, x0 + w - 1 + (ar ? ext : 0)) : ax0[q] - 1;
-    ly0[q] = y0 - availU;
-    ly1[q] = availL ? imin(maxY, y0 + h - 1 + (bl ? ext : 0)) : ly0[q] - 1;
-    ur[2 * q] = (ay[q] << sub) >> 2;
-    uc[2 * q] = (ax0[q] << sub) >> 2;
-    urow[2 * q] = 1;
-    un[2 * q] = ax1[q] >= ax0[q] ? ((ax1[q] << sub) >> 2) - uc[2 * q] + 1 : 0;
-    ur[2 * q + 1] = (ly0[q] << sub) >> 2;
-    uc[2 * q + 1] = ((x0 - 1) << sub) >> 2;
-    urow[2 * q + 1] = 0;
-    un[2 * q + 1] = ly1[q] >= ly0[q] ? ((ly1[q] << sub) >> 2) - ur[2 * q + 1] + 1 : 0;
+    int p = p0 + q;
+    EdgeRuns e = edge_runs(fp, b, p, sm.cornerAR[p], sm.cornerBL[p]);
+    ay[q] = e.ay;
+    ax0[q] = e.ax0;
+    ax1[q] = e.ax1;
+    ly0[q] = e.ly0;
+    ly1[q] = e.ly1;
+    for (int k = 0; k < 2; k++) {
+      ur[2 * q + k] = e.ur[k];
+      uc[2 * q + k] = e.uc[k];
+      urow[2 * q + k] = e.urow[k];
+      un[2 * q + k] = e.un[k];
+    }
   }
-  wait_units(c, sm, group, ur, uc, urow, un);
+  // luma: the ready queue hands out a block only once every block its luma
+  // edges read has published its luma (k_block_deps); chroma: wait here
+  if (group) wait_units(c, sm, group, ur, uc, urow, un);
   __threadfence();
   __syncthreads();
   CopySeg sg[4];
@@ -942,6 +990,26 @@ __device__ void predict_block(Smem &sm, const pred::Inter &ip, int lw, int h, in
   __syncthreads();
 }
 
+#define MAX_SUCC 96  // successors per block: at most 25 along each edge, with margin
+
+// Appends a block whose luma dependencies are complete to the ready queue.
+__device__ __forceinline__ void push_ready(const Ctx &c, int blk) {
+  int t = atomicAdd(c.qtail, 1);
+  c.queue[t] = blk;
+  __threadfence();
+  atomicExch(c.qvalid + t, 1);
+}
+
+// After this block's luma is published: one dependency fewer for each
+// successor; the last one releases it to the ready queue.
+__device__ void release_successors(const Ctx &c, const Smem &sm) {
+  int n = imin(c.succ_count[sm.me], MAX_SUCC);
+  for (int k = threadIdx.x; k < n; k += RT) {
+    int s = c.succ[sm.me * MAX_SUCC + k];
+    if (atomicSub(c.dep_count + s, 1) == 1) push_ready(c, s);
+  }
+}
+
 // One block (recon_block, k_recon.h:293-394); sm.blk holds it.
 template <bool INTER>
 __device__ void recon_block(const Ctx &c, Smem &sm, BlockInfo *gb) {
@@ -1007,6 +1075,7 @@ __device__ void recon_block(const Ctx &c, Smem &sm, BlockInfo *gb) {
       // luma is final: publish it, so blocks waiting only on it go ahead
       // while this one codes its chroma
       unstage_intra(c, sm, 0, 1);
+      release_successors(c, sm);
       stage_edges(c, sm, 1);
     }
     int sub = plane > 0, stride = fp->stride[plane];
@@ -1165,6 +1234,65 @@ __global__ void __launch_bounds__(INTER_THREADS, 2) k_recon_inter(Ctx cg) {
   }
 }
 
+// Per frame, after the claim list: each intra block's dependencies (one
+// warp per block). The blocks under its luma and chroma edge samples
+// (edge_runs with its corner units' BlockDecoded) that are intra and not
+// itself, without repeats: their number is its dependency count, and it
+// joins each one's successor list. A block is released once all of them
+// have published their luma; by then each of them is held by a worker, so
+// the chroma waits that follow always end. Blocks with none start in the
+// ready queue.
+__global__ void __launch_bounds__(128) k_block_deps(Ctx c, const int *list, const int *total) {
+  __shared__ int cand[4][160];
+  const FrameParams *fp = c.fp;
+  int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int item = blockIdx.x * 4 + warp; item < *total; item += gridDim.x * 4) {
+    int me = list[item];
+    BlockInfo b = c.blocks[me];
+    int sb = me / MAX_BLOCKS_PER_SB, r0 = (sb / fp->sb_cols) * 16, c0 = (sb % fp->sb_cols) * 16;
+    EdgeRuns e[2];  // luma; chroma (both chroma planes share their geometry)
+    for (int p = 0; p < 2; p++)
+      e[p] = edge_runs(fp, b, p, corner_decoded(fp, c.blk_at, b, me, r0, c0, p, 0),
+                       corner_decoded(fp, c.blk_at, b, me, r0, c0, p, 1));
+    int run[4] = {e[0].un[0], e[0].un[1], e[1].un[0], e[1].un[1]};
+    int n = imin(160, run[0] + run[1] + run[2] + run[3]);
+    int nblk = fp->sb_cols * fp->sb_rows * MAX_BLOCKS_PER_SB;
+    for (int i = lane; i < n; i += 32) {
+      int k = 0, j = i;
+      while (j >= run[k]) j -= run[k++];
+      const EdgeRuns &er = e[k >> 1];
+      int kk = k & 1;
+      int r = er.ur[kk] + (er.urow[kk] ? 0 : j), col = er.uc[kk] + (er.urow[kk] ? j : 0);
+      int d = c.blk_at[r * fp->mi_cols + col];
+      if (d == me || (unsigned)d >= (unsigned)nblk || c.blocks[d].is_inter) d = -1;
+      cand[warp][i] = d;
+    }
+    __syncwarp();
+    int cnt = 0;
+    for (int i = lane; i < n; i += 32) {
+      int d = cand[warp][i];
+      if (d < 0) continue;
+      bool dup = false;
+      for (int j = 0; j < i && !dup; j++) dup = cand[warp][j] == d;
+      if (dup) continue;
+      cnt++;
+      int slot = atomicAdd(c.succ_count + d, 1);
+      if (slot < MAX_SUCC) {
+        c.succ[d * MAX_SUCC + slot] = me;
+      } else {
+        atomicExch(c.status, 2);
+        atomicExch(c.status + 1, 1);
+      }
+    }
+    for (int off = 16; off > 0; off >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, off);
+    if (lane == 0) {
+      if (cnt == 0) push_ready(c, me);
+      else c.dep_count[me] = cnt;
+    }
+    __syncwarp();
+  }
+}
+
 // Claim state of the recon launch: the list, its length and the counter.
 struct Claim {
   const int *list;
@@ -1184,8 +1312,23 @@ __global__ void __launch_bounds__(INTRA_THREADS, 1) k_recon_blocks(Ctx cg, Claim
   int total = *q.total;
   for (;;) {
     if (threadIdx.x == 0) {
-      int item = vstatus[1] ? total : atomicAdd(q.next, 1);
-      int me = item < total ? q.list[item] : -1;
+      int slot = vstatus[1] ? total : atomicAdd(q.next, 1), me = -1;
+      if (slot < total) {
+        // the slot fills once its block is released (every block is, once
+        // the blocks before it in any dependency chain complete)
+        volatile int *vvalid = c.qvalid + slot;
+        int spins = 0;
+        while (!*vvalid && !vstatus[1]) {
+          if (++spins > SPIN_LIMIT) {
+            atomicExch(c.status, 1);
+            atomicExch(c.status + 1, 1);
+            break;
+          }
+          __nanosleep(64);
+        }
+        __threadfence();
+        if (*vvalid) me = ((volatile int *)c.queue)[slot];
+      }
       sm.flag = me;
       if (me >= 0) {
         int sb = me / MAX_BLOCKS_PER_SB;

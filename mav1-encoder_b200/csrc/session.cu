@@ -72,11 +72,12 @@ struct mav1cu_session {
   int mats_dirty;          // MATS changed since mats_t was derived
   int mats_exposed;        // MATS's device address was handed out: derive mats_t before every recon
   int *waves;              // superblocks in wave order
-  int *status;             // device status: [0] error, [1] abort, [2] claim counter, [3] claim list length
+  int *status;             // device status: [0] error, [1] abort, [2] queue head, [3] intra blocks, [4] queue tail
   int *blk_at;             // block index per 4x4 luma unit
   int *blk_list;           // recon claim list
   int *blk_done;           // per-block completion flags of the recon launch: luma, then chroma
-  int resident_recon;      // recon workers (one-warp CTAs) resident at once
+  int *dep_count, *succ_count, *succ, *queue, *qvalid;  // intra ready queue (rec::Ctx)
+  int resident_recon;      // intra recon workers (CTAs, one per SM)
   std::vector<int> wave_start, wave_len;
   int wave_tile_w;
   FrameParams fp;          // host copy of the current parameters
@@ -235,7 +236,7 @@ static void free_all(mav1cu_session *s) {
   for (int i = 0; i < MAV1CU_BUF_COUNT; i++)
     if (s->buf[i]) cudaFree(s->buf[i]);
   void *extra[] = {s->qp[0], s->qp[1], s->dsrc, s->dref[0], s->dref[1], s->ys, s->uvs, s->waves, s->status, s->blk_at, s->blk_list,
-                   s->blk_done, s->mats_t};
+                   s->blk_done, s->mats_t, s->dep_count, s->succ_count, s->succ, s->queue, s->qvalid};
   for (void *p : extra)
     if (p) cudaFree(p);
   if (s->own_stream) cudaStreamDestroy(s->own_stream);
@@ -281,9 +282,15 @@ extern "C" int mav1cu_session_create(int width, int height, int max_cdef_presets
   if (e == cudaSuccess) e = cudaMalloc(&s->ys, (size_t)g.mi_rows * g.mi_cols);
   if (e == cudaSuccess) e = cudaMalloc(&s->uvs, (size_t)g.mi_rows * g.mi_cols);
   if (e == cudaSuccess) e = cudaMalloc(&s->waves, sizeof(int) * nsb);
-  if (e == cudaSuccess) e = cudaMalloc(&s->status, sizeof(int) * 4);
+  if (e == cudaSuccess) e = cudaMalloc(&s->status, sizeof(int) * 8);
   if (e == cudaSuccess) e = cudaMalloc(&s->blk_at, sizeof(int) * g.mi_rows * g.mi_cols);
   if (e == cudaSuccess) e = cudaMalloc(&s->mats_t, sizeof(int32_t) * 4096 * 15);
+  size_t nblk = MAX_BLOCKS_PER_SB * nsb;
+  if (e == cudaSuccess) e = cudaMalloc(&s->dep_count, sizeof(int) * nblk);
+  if (e == cudaSuccess) e = cudaMalloc(&s->succ_count, sizeof(int) * nblk);
+  if (e == cudaSuccess) e = cudaMalloc(&s->succ, sizeof(int) * nblk * MAX_SUCC);
+  if (e == cudaSuccess) e = cudaMalloc(&s->queue, sizeof(int) * nblk);
+  if (e == cudaSuccess) e = cudaMalloc(&s->qvalid, sizeof(int) * nblk);
   s->mats_dirty = 1;
   if (e == cudaSuccess) e = cudaMalloc(&s->blk_list, sizeof(int) * MAX_BLOCKS_PER_SB * nsb);
   if (e == cudaSuccess) e = cudaMalloc(&s->blk_done, 2 * sizeof(int) * MAX_BLOCKS_PER_SB * nsb);
@@ -295,7 +302,7 @@ extern "C" int mav1cu_session_create(int width, int height, int max_cdef_presets
     return e == cudaErrorMemoryAllocation ? MAV1CU_ERR_NOMEM : MAV1CU_ERR_CUDA;
   }
   s->stream = s->own_stream;
-  cudaMemset(s->status, 0, sizeof(int) * 4);
+  cudaMemset(s->status, 0, sizeof(int) * 8);
   cudaMemset(s->blk_at, 0xff, sizeof(int) * g.mi_rows * g.mi_cols);  // -1: no block
   std::vector<int32_t> mats(4096 * 15);
   mav1cu_build_fwd_matrices(mats.data());
@@ -313,7 +320,9 @@ extern "C" int mav1cu_session_create(int width, int height, int max_cdef_presets
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, rec::k_recon_blocks, rec::INTRA_THREADS, sizeof(rec::Smem));
-    s->resident_recon = imax(1, sms * imax(1, per));
+    // one worker per SM: the ready queue keeps them on ready blocks, and the
+    // rest of each SM stays free for the other engines' kernels
+    s->resident_recon = imax(1, sms * imin(1, imax(1, per)));
   }
   cudaFuncSetAttribute(ana::k_analyze_level, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ANA_SMEM);
   *out = s;
@@ -527,7 +536,21 @@ extern "C" int mav1cu_recon(mav1cu_session *s) {
   if (after_launch(s, "recon unit map")) return s->err;
   rec::k_block_order<<<1, 1024, 0, s->stream>>>(c.blocks, c.sbs, s->waves, nsb, s->blk_list, s->status + 3);
   if (after_launch(s, "recon claim list")) return s->err;
-  if (check_cuda(s, cudaMemsetAsync(s->status + 2, 0, sizeof(int), s->stream), "recon counter")) return s->err;
+  size_t nblk = (size_t)MAX_BLOCKS_PER_SB * nsb;
+  if (check_cuda(s, cudaMemsetAsync(s->succ_count, 0, sizeof(int) * nblk, s->stream), "recon successors") ||
+      check_cuda(s, cudaMemsetAsync(s->qvalid, 0, sizeof(int) * nblk, s->stream), "recon queue") ||
+      check_cuda(s, cudaMemsetAsync(s->status + 2, 0, sizeof(int), s->stream), "recon queue head") ||
+      check_cuda(s, cudaMemsetAsync(s->status + 4, 0, sizeof(int), s->stream), "recon queue tail"))
+    return s->err;
+  c.dep_count = s->dep_count;
+  c.succ_count = s->succ_count;
+  c.succ = s->succ;
+  c.queue = s->queue;
+  c.qvalid = s->qvalid;
+  c.qtail = s->status + 4;
+  rec::k_block_deps<<<(unsigned)imin((int)((nblk + 3) / 4), 4 * s->resident_recon), 128, 0, s->stream>>>(
+      c, s->blk_list, s->status + 3);
+  if (after_launch(s, "recon dependencies")) return s->err;
   rec::Claim q;
   q.list = s->blk_list;
   q.total = s->status + 3;
@@ -599,7 +622,9 @@ extern "C" int mav1cu_synchronize(mav1cu_session *s) {
   if (check_cuda(s, cudaStreamSynchronize(s->stream), "synchronize")) return s->err;
   int st[2] = {0, 0};
   if (check_cuda(s, cudaMemcpy(st, s->status, sizeof st, cudaMemcpyDeviceToHost), "status")) return s->err;
-  if (st[0]) return set_error(s, MAV1CU_ERR_DEVICE, "device status %d: a recon dependency wait gave up", st[0]);
+  if (st[0])
+    return set_error(s, MAV1CU_ERR_DEVICE, "device status %d: %s", st[0],
+                     st[0] == 2 ? "a recon successor list overflowed" : "a recon dependency wait gave up");
   return MAV1CU_OK;
 }
 
