@@ -202,24 +202,50 @@ def run_ours(args, rank, world):
         t = torch.tensor([per_step, per_e2e, per_seq], dtype=torch.float64, device=f"cuda:{dev}")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         per_step, per_e2e, per_seq = t.tolist()
-    kern = kernel_times(streams[0].session, S, None) if (rank == 0 and not args.no_roofline) else None
+    kern = kernel_times(streams[0].session, S, frames_dev) if (rank == 0 and not args.no_roofline) else None
     for st in streams:
         st.close()
     return dict(ms=per_step, ms_e2e=per_e2e, ms_seq=per_seq, launches=nlaunch, clocks=clk.summary(),
                 h2d=SPEC.frames * fbytes, d2h=d2h_per_step, kern=kern, gops=len(gops))
 
 
-def kernel_times(sess, stream, step_fn):
-    """Per-kernel device time of one step, measured with CUDA events around
-    each stage of one ALTREF frame (the dominant frame kind) on the session
-    stream; used for the roofline of the dominant kernel."""
+def kernel_times(sess, stream, frames_dev):
+    """Device times for the roofline, with CUDA events on the stream the
+    kernels are launched on.
+
+    dominant: the reconstruction stage of the clip's first key frame, which is
+    the dominant kernel k_recon_blocks (the intra block workers, 29% of the
+    clip's device time in the ncu launch list) plus four short set-up launches.
+    A fresh stream codes the key frame, then the stage is re-run on the engine
+    session that holds the frame's analysis output (recon reproduces its
+    outputs from the same inputs). stage_ms: every stage of one ALTREF frame,
+    for reference."""
     import torch
     import mav1cu
 
-    # re-run one ALTREF frame stage by stage with events between stages
-    sess.set_stream(stream.cuda_stream)
     cfg = mav1cu.cli_config(SPEC.width, SPEC.height, **FLAGS)
     jobs = mav1cu.plan(cfg, SPEC.frames)
+    key = jobs[0]
+    st = mav1cu.Stream(cfg)
+    st.encode(key, frames_dev[key["disp"]].data_ptr(), True)
+    st.synchronize()
+    es = st.engines[st.engine_of(key)]
+    ext = torch.cuda.ExternalStream(st.lib.mav1cu_get_stream(es.h))
+    ts = []
+    for i in range(8):
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        ev[0].record(ext)
+        es.recon()
+        ev[1].record(ext)
+        ev[1].synchronize()
+        if i >= 3:
+            ts.append(ev[0].elapsed_time(ev[1]))
+    es.synchronize()
+    key_recon_ms = statistics.median(ts)
+    st.close()
+
+    # every stage of one ALTREF frame (inputs: whatever the session holds)
+    sess.set_stream(stream.cuda_stream)
     arf = next(j for j in jobs if j["kind"] == 1)
     fp, presets = mav1cu.frame_params(cfg, arf)
     sess.set_params(fp)
@@ -234,40 +260,41 @@ def kernel_times(sess, stream, step_fn):
         stream.synchronize()
         for name, fn in stages:
             ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
-            ts = []
+            tt = []
             for _ in range(5):
                 ev[0].record(stream)
                 fn()
                 ev[1].record(stream)
                 ev[1].synchronize()
-                ts.append(ev[0].elapsed_time(ev[1]))
-            res[name] = statistics.median(ts)
-    return res
+                tt.append(ev[0].elapsed_time(ev[1]))
+            res[name] = statistics.median(tt)
+    return {"key_recon_ms": key_recon_ms, "arf_stage_ms": res}
+
+
+# Bytes the key-frame reconstruction must move at 1080p, each once: source
+# read (3,133,440), reconstruction written (3,133,440), block records read and
+# written (510 superblocks x 64 x 108 bytes, twice), coefficients written
+# (510 x 6144 x 4), forward matrices read (61,440 x 4).
+KEY_RECON_BYTES = 2 * 3133440 + 2 * 510 * 64 * 108 + 510 * 6144 * 4 + 61440 * 4
+# dram__bytes_read.sum + dram__bytes_write.sum of that launch of k_recon_blocks
+# in one ncu capture (the key frame of `bench.py --profile-frames 3`).
+KEY_RECON_DRAM_BYTES = 15770000
 
 
 def roofline(kern, peaks):
-    """Roofline of the dominant stage of an ALTREF frame: algorithmic bytes
-    (compulsory reads + writes of the stage at 1080p) over its measured time."""
+    """Roofline of the dominant kernel (k_recon_blocks) through its stage on
+    the key frame: algorithmic bytes over the measured stage time, against the
+    measured HBM copy bandwidth. The kernel is a dependency chain (latency
+    bound), so the fraction is small by nature."""
     if not kern:
         return None
-    name = max(kern, key=kern.get)
-    fb = 3133440  # padded 1080p frame bytes
-    nsb = 510
-    alg = {  # compulsory bytes per launch of each stage at 1080p: frames read or written once, tables once
-        "motion_search": 3 * fb + 16 * 1920 * 1080 + nsb * 85 * 8,
-        "analyze": 3 * fb + nsb * 85 * 13 * (8 + 108) // 13 + nsb * 64 * 108,
-        "edge_types": 2 * nsb * 64 * 108,
-        "recon": 3 * fb + nsb * 64 * 108 + nsb * 6144 * 4 + 61440 * 4,
-        "filter_info": nsb * 64 * 108 + 135 * 480,
-        "filter": 2 * fb + 2 * fb + 135 * 480,
-        "cdef_select": 4 * fb + fb,
-    }[name]
-    t = kern[name] * 1e-3
+    t = kern["key_recon_ms"] * 1e-3
     peak = peaks.get("hbm_gbs", 6650.0)
-    achieved = alg / t / 1e9
-    return {"bound": "hbm", "kernel": name, "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-            "frac": round(achieved / peak, 5), "traffic": None, "algorithmic_bytes": alg,
-            "ms_per_launch": round(kern[name], 4), "stage_ms": {k: round(v, 4) for k, v in kern.items()},
+    achieved = KEY_RECON_BYTES / t / 1e9
+    return {"bound": "hbm", "kernel": "k_recon_blocks (key-frame recon stage)", "achieved": round(achieved, 2),
+            "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 6), "traffic": KEY_RECON_DRAM_BYTES,
+            "algorithmic_bytes": KEY_RECON_BYTES, "ms_per_launch": round(kern["key_recon_ms"], 3),
+            "arf_stage_ms": {k: round(v, 4) for k, v in kern["arf_stage_ms"].items()},
             "peak_source": "MEASURED_PEAKS.json" if "hbm_gbs" in peaks else "fallback"}
 
 
