@@ -198,6 +198,80 @@ __device__ void inv_col(Smem &sm, int j, int w, int ck, int fud, int flr, uint8_
   }
 }
 
+// The 32- and 64-point DCT rows / columns by two threads each (adjacent
+// lanes of one warp; half 0 runs the even half and the first join pairs,
+// half 1 the odd half and the rest, tx::idct_odd), which halves the
+// sequential butterfly chain of the largest transforms. Each thread loads
+// its permuted inputs directly; the pre-join halves meet in sm.resid.
+template <int LW>
+__device__ void inv_row_split(Smem &sm, const int32_t *q, int i, int half, int th, int dcQ, int acQ, int denom,
+                              int rect, int rowShift) {
+  constexpr int W = 1 << LW, HW = W / 2, TW = W < 32 ? W : 32;
+  unsigned pair = 3u << ((threadIdx.x & 31) & ~1u);
+  int32_t t[HW];
+  int nz = 0;
+#pragma unroll
+  for (int k = 0; k < HW; k++) {
+    int j = tx::brev(LW, k + half * HW);
+    t[k] = (j < TW && i < th) ? tx::dequant_level(q[i * TW + j], (i == 0 && j == 0) ? dcQ : acQ, denom) : 0;
+    nz |= t[k];
+  }
+  nz |= __shfl_xor_sync(pair, nz, 1);
+  int32_t *row = sm.resid + i * 64;
+  if (!nz) {
+#pragma unroll
+    for (int k = 0; k < HW; k++) row[k + half * HW] = 0;
+    return;
+  }
+  if (rect) {
+#pragma unroll
+    for (int k = 0; k < HW; k++) t[k] = (int32_t)round2l((int64_t)t[k] * 2896, 12);
+  }
+  if (half == 0) tx::idct<LW - 1, false>(t, 16);
+  else tx::idct_odd<LW>(t - HW, 16);
+#pragma unroll
+  for (int k = 0; k < HW; k++) row[k + half * HW] = t[k];
+  __syncwarp(pair);
+#pragma unroll
+  for (int k = 0; k < HW / 2; k++) {
+    int a = k + half * (HW / 2), b = W - 1 - a;
+    int32_t va = row[a], vb = row[b];
+    tx::idct_join_pair(&va, &vb, 16);
+    row[a] = clip3(-(1 << 15), (1 << 15) - 1, round2(va, rowShift));
+    row[b] = clip3(-(1 << 15), (1 << 15) - 1, round2(vb, rowShift));
+  }
+}
+
+template <int LH>
+__device__ void inv_col_split(Smem &sm, int j, int half, int w, int fud, int flr, uint8_t *rec, int rs, int x, int y) {
+  constexpr int H = 1 << LH, HH = H / 2;
+  unsigned pair = 3u << ((threadIdx.x & 31) & ~1u);
+  int32_t t[HH];
+#pragma unroll
+  for (int k = 0; k < HH; k++) t[k] = sm.resid[tx::brev(LH, k + half * HH) * 64 + j];
+  __syncwarp(pair);  // both halves read before the column is overwritten
+  if (half == 0) tx::idct<LH - 1, false>(t, 16);
+  else tx::idct_odd<LH>(t - HH, 16);
+#pragma unroll
+  for (int k = 0; k < HH; k++) sm.resid[(k + half * HH) * 64 + j] = t[k];
+  __syncwarp(pair);
+  uint8_t *col = rec ? rec + y * rs + x + (flr ? (w - 1 - j) : j) : nullptr;
+#pragma unroll
+  for (int k = 0; k < HH / 2; k++) {
+    int a = k + half * (HH / 2), b = H - 1 - a;
+    int32_t va = sm.resid[a * 64 + j], vb = sm.resid[b * 64 + j];
+    tx::idct_join_pair(&va, &vb, 16);
+    if (rec) {
+      uint8_t *oa = col + (fud ? (H - 1 - a) : a) * rs, *ob = col + (fud ? (H - 1 - b) : b) * rs;
+      *oa = (uint8_t)clip1((int)*oa + round2(va, 4));
+      *ob = (uint8_t)clip1((int)*ob + round2(vb, 4));
+    } else {
+      sm.resid[a * 64 + j] = round2(va, 4);
+      sm.resid[b * 64 + j] = round2(vb, 4);
+    }
+  }
+}
+
 // Levels of a candidate -> reconstruction residual (spec 7.13.3 with the
 // dequantisation of 7.12.3), into sm.resid (stride 64).
 // With rec set, the column pass adds its output straight into the
@@ -213,7 +287,12 @@ __device__ __forceinline__ void inverse_2d_upto(Smem &sm, const int32_t *q, int 
   int rowShift = T(Transform_Row_Shift)[txSz], denom = tx::dq_denom(txSz);
   int rect = iabs(lw - lh) == 1;
   int rk = tx::row_kind(txType), ck = tx::col_kind(txType);
-  for (int i = threadIdx.x; i < h; i += RT) {
+  if (MAXL >= 5 && lw >= 5 && rk == tx::KIND_DCT) {
+    for (int p = threadIdx.x; p < 2 * h; p += RT) {
+      if (lw == 5) inv_row_split<5>(sm, q, p >> 1, p & 1, th, dcQ, acQ, denom, rect, rowShift);
+      else inv_row_split<6>(sm, q, p >> 1, p & 1, th, dcQ, acQ, denom, rect, rowShift);
+    }
+  } else for (int i = threadIdx.x; i < h; i += RT) {
     switch (lw) {
       case 2: inv_row<2>(sm, q, i, th, dcQ, acQ, denom, rect, rk, rowShift); break;
       case 3: inv_row<3>(sm, q, i, th, dcQ, acQ, denom, rect, rk, rowShift); break;
@@ -224,7 +303,12 @@ __device__ __forceinline__ void inverse_2d_upto(Smem &sm, const int32_t *q, int 
   }
   __syncthreads();
   int fud = tx::flip_ud(txType), flr = tx::flip_lr(txType);
-  for (int j = threadIdx.x; j < w; j += RT) {
+  if (MAXL >= 5 && lh >= 5 && ck == tx::KIND_DCT) {
+    for (int p = threadIdx.x; p < 2 * w; p += RT) {
+      if (lh == 5) inv_col_split<5>(sm, p >> 1, p & 1, w, fud, flr, rec, rs, x, y);
+      else inv_col_split<6>(sm, p >> 1, p & 1, w, fud, flr, rec, rs, x, y);
+    }
+  } else for (int j = threadIdx.x; j < w; j += RT) {
     switch (lh) {
       case 2: inv_col<2>(sm, j, w, ck, fud, flr, rec, rs, x, y); break;
       case 3: inv_col<3>(sm, j, w, ck, fud, flr, rec, rs, x, y); break;

@@ -48,14 +48,16 @@ HD void H(int32_t *t, int a, int b, int flip, int r) {
 }
 
 // Inverse DCT of length 1 << N (spec 7.13.2.3).
-template <int N>
+template <int N, bool PERM = true>
 HD void idct(int32_t *t, int r) {
   constexpr int n0 = 1 << N;
-  int32_t c[n0];
+  if (PERM) {
+    int32_t c[n0];
 #pragma unroll
-  for (int i = 0; i < n0; i++) c[i] = t[i];
+    for (int i = 0; i < n0; i++) c[i] = t[i];
 #pragma unroll
-  for (int i = 0; i < n0; i++) t[i] = c[brev(N, i)];
+    for (int i = 0; i < n0; i++) t[i] = c[brev(N, i)];
+  }
   if (N == 6) {
 #pragma unroll
     for (int i = 0; i < 16; i++) B(t, 32 + i, 63 - i, 63 - 4 * brev(4, i), 0);
@@ -191,6 +193,78 @@ HD void idct(int32_t *t, int r) {
 }
 
 // ADST input / output permutations (spec 7.13.2.4, 7.13.2.5).
+// The 2^N-point inverse DCT (N = 5, 6) as two halves and a join, for two
+// threads. After the input permutation, the operations of idct<N> on
+// elements 0 .. n0/2 - 1 are exactly idct<N - 1> without its permutation,
+// and those on n0/2 .. n0 - 1 are the groups that only N adds (idct_odd,
+// the same operations in the same order; t points at element 0, so the odd
+// half is t[n0/2 ..]); the halves touch disjoint elements until the last
+// stage, H(i, n0 - 1 - i) for i < n0/2 (idct_join_pair). Running the
+// halves concurrently and then the join gives idct<N>'s result exactly.
+template <int N>
+HD void idct_odd(int32_t *t, int r) {
+  if (N == 6) {
+#pragma unroll
+    for (int i = 0; i < 16; i++) B(t, 32 + i, 63 - i, 63 - 4 * brev(4, i), 0);
+#pragma unroll
+    for (int i = 0; i < 16; i++) H(t, 32 + i * 2, 33 + i * 2, i & 1, r);
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+#pragma unroll
+      for (int j = 0; j < 2; j++) B(t, 62 - i * 4 - j, 33 + i * 4 + j, 60 - 16 * brev(2, i) + 64 * j, 1);
+#pragma unroll
+    for (int i = 0; i < 8; i++)
+#pragma unroll
+      for (int j = 0; j < 2; j++) H(t, 32 + i * 4 + j, 35 + i * 4 - j, i & 1, r);
+#pragma unroll
+    for (int i = 0; i < 2; i++)
+#pragma unroll
+      for (int j = 0; j < 4; j++) B(t, 61 - i * 8 - j, 34 + i * 8 + j, 56 - i * 32 + (j >> 1) * 64, 1);
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+#pragma unroll
+      for (int j = 0; j < 4; j++) H(t, 32 + 8 * i + j, 39 + 8 * i - j, i & 1, r);
+#pragma unroll
+    for (int i = 0; i < 8; i++) B(t, 59 - i, 36 + i, i < 4 ? 48 : 112, 1);
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+      H(t, 32 + i, 47 - i, 0, r);
+      H(t, 48 + i, 63 - i, 1, r);
+    }
+#pragma unroll
+    for (int i = 0; i < 8; i++) B(t, 55 - i, 40 + i, 32, 1);
+  } else {
+#pragma unroll
+    for (int i = 0; i < 8; i++) B(t, 16 + i, 31 - i, 6 + (brev(3, 7 - i) << 3), 0);
+#pragma unroll
+    for (int i = 0; i < 8; i++) H(t, 16 + 2 * i, 17 + 2 * i, i & 1, r);
+#pragma unroll
+    for (int i = 0; i < 2; i++)
+#pragma unroll
+      for (int j = 0; j < 2; j++) B(t, 30 - 4 * i - j, 17 + 4 * i + j, 24 + (j << 6) + ((1 - i) << 5), 1);
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+#pragma unroll
+      for (int j = 0; j < 2; j++) H(t, 16 + 4 * i + j, 19 + 4 * i - j, i & 1, r);
+#pragma unroll
+    for (int i = 0; i < 4; i++) B(t, 29 - i, 18 + i, 48 + (i >> 1) * 64, 1);
+#pragma unroll
+    for (int i = 0; i < 2; i++)
+#pragma unroll
+      for (int j = 0; j < 4; j++) H(t, 16 + i * 8 + j, 23 + i * 8 - j, i, r);
+#pragma unroll
+    for (int i = 0; i < 4; i++) B(t, 27 - i, 20 + i, 32, 1);
+  }
+}
+
+// One pair of the join stage: H(i, n0 - 1 - i) with the clamp to r bits.
+HD void idct_join_pair(int32_t *a, int32_t *b, int r) {
+  int32_t x = *a, y = *b;
+  int lo = -(1 << (r - 1)), hi = (1 << (r - 1)) - 1;
+  *a = clip3(lo, hi, x + y);
+  *b = clip3(lo, hi, x - y);
+}
+
 template <int N>
 HD void adst_in_perm(int32_t *t) {
   constexpr int n0 = 1 << N;

@@ -97,3 +97,20 @@ def test_plan_turbo_gop_structure():
         kinds[k] = kinds.get(k, 0) + 1
     assert kinds == {"key": 2, "arf": 58, "leaf": 58, "regular": 2}
     assert sorted(int(j["disp"]) for j in jobs) == list(range(120))
+
+
+def test_split_large_inverse_dct_is_exact(tmp_path):
+    """The two-thread form of the 32- and 64-point inverse DCT equals the
+    spec-order butterfly list on the host (tests/native/idct_split_check.cpp)."""
+    import shutil
+    import subprocess
+    cxx = shutil.which("g++")
+    if cxx is None:
+        pytest.skip("no host C++ compiler")
+    exe = tmp_path / "idct_split_check"
+    subprocess.run([cxx, "-O2", "-std=c++17", "-I", os.path.join(ROOT, "include"),
+                    "-I", os.path.join(ROOT, "mav1-encoder_b200", "csrc"), "-x", "c++",
+                    os.path.join(ROOT, "tests", "native", "idct_split_check.cpp"), "-o", str(exe)],
+                   check=True, capture_output=True)
+    r = subprocess.run([str(exe)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stdout + r.stderr
