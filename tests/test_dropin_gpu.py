@@ -20,6 +20,10 @@ CASES = {
     "lowdelay_lr": (synthetic.ClipSpec(150, 102, 5, seed=32, rects=2, rect_size=(16, 40)), 5,
                     dict(q=200, golden=1, keyint=4, lr_test=1)),
     "lossless": (synthetic.ClipSpec(96, 64, 3, seed=33, rects=1, rect_size=(16, 32)), 3, dict(q=0, fast=1)),
+    # the benchmark clip and flags at full size (key, ALTREF, leaf and a second key frame)
+    "c1_1080p_turbo": (synthetic.CONFIGS["c1_1080p"], 9, dict(q=125, turbo=1, keyint=8, tiles=2)),
+    # the 4K clip's geometry (3 tile columns) with the turbo tool set
+    "c2_2160p_turbo": (synthetic.CONFIGS["c2_2160p"], 3, dict(q=125, turbo=1, tiles=3)),
 }
 
 

@@ -19,6 +19,31 @@ CASES = {
 }
 
 
+class _WriterTrace(oracle.Trace):
+    """Only what the stream comparison reads (keeps a 1080p trace small)."""
+    CAPTURE = {
+        oracle.STAGE["PARAMS"]: ["PARAMS"],
+        oracle.STAGE["ANALYZE"]: ["SBS"],
+        oracle.STAGE["RECON"]: ["BLOCKS", "COEFS"],
+        oracle.STAGE["CDEFSEL"]: ["CDEF_CHOICE"],
+        oracle.STAGE["DONE"]: ["REC"],
+    }
+
+
+@pytest.mark.skipif(not oracle.available(), reason="oracle not built")
+def test_stream_matches_oracle_1080p():
+    """The benchmark's clip and flags at full size through the device stream:
+    key, ALTREF and leaf frames and a second key frame (keyint 8)."""
+    spec, n = synthetic.CONFIGS["c1_1080p"], 9
+    flags = dict(q=125, turbo=1, keyint=8, tiles=2)
+    frames = list(synthetic.generate(spec, n))
+    tr = _WriterTrace()
+    oracle.encode(frames, oracle.cli_config(spec.width, spec.height, **flags), trace=tr)
+    res = parity.stream_vs_oracle(tr, frames, flags, spec)
+    bad = [(k, o) for k, o in res if any(o.values())]
+    assert not bad, bad
+
+
 @pytest.mark.skipif(not oracle.available(), reason="oracle not built")
 @pytest.mark.parametrize("name", sorted(CASES))
 def test_stream_matches_oracle(name):
