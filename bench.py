@@ -15,9 +15,13 @@ not part of this path) are not timed.
 value: frames/s with the source frames resident in HBM (CUDA events on the
        session stream, max over ranks).
 e2e:   the same through the C ABI from pinned host memory: every frame's
-       source is copied host->device and its entropy-coder inputs (blocks,
-       superblock table, coefficients, CDEF choices) plus the shown frames'
-       reconstructions are copied device->host inside the timed region.
+       source is copied host->device, its entropy-coder inputs (superblock
+       table, CDEF choices, the blocks in use, the levels of coded planes)
+       are packed on the device and stored into mapped pinned host memory
+       (mav1cu_export), and the shown frames' reconstructions are copied
+       device->host, all inside the timed region. d2h_bytes_per_step counts
+       the bytes each frame's export image holds (its header's byte count,
+       read in an untimed pass over the same step) plus the reconstructions.
 --impl reference: the reference encoder's own scalar CPU path (oracle/_ref,
        built from the reference sources) on the host cores, all threads.
 
@@ -133,10 +137,12 @@ def run_ours(args, rank, world):
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{dev}")
     pinned = torch.from_numpy(frames_host).pin_memory()
     geom = mav1cu.geometry(SPEC.width, SPEC.height)
-    sizes = {b: streams[0].session.size(b) for b in ("BLOCKS", "SBS", "COEFS", "CDEF_CHOICE")}
-    sizes["REC"] = geom["frame_bytes"]
-    out_bufs = {b: torch.empty(n, dtype=torch.uint8).pin_memory() for b, n in sizes.items()}
-    d2h_per_step = 0
+    rec_out = torch.empty(geom["frame_bytes"], dtype=torch.uint8).pin_memory()
+    # one export image per engine of each GOP stream: a frame's image stays
+    # intact until that engine's next frame
+    cap = streams[0].session.export_capacity()
+    images = {(g, k): torch.empty(cap, dtype=torch.uint8).pin_memory()
+              for g in range(len(gops)) for k in range(len(streams[0].engines))}
 
     def step_device(order=order):
         for g, j in order:
@@ -145,15 +151,28 @@ def run_ours(args, rank, world):
     def step_sequential():
         step_device(seq_order)
 
+    def e2e_frame(g, j):
+        sess = streams[g].encode(j, pinned[j["disp"]].data_ptr(), False)
+        img = images[(g, mav1cu.Stream.engine_of(j))]
+        sess.export(img.data_ptr(), cap)
+        if not j["hidden"]:
+            sess.lib.mav1cu_download(sess.h, mav1cu.BUF["REC"], rec_out.data_ptr(), geom["frame_bytes"])
+        return img
+
     def step_e2e():
-        nonlocal d2h_per_step
-        d2h = 0
         for g, j in order:
-            sess = streams[g].encode(j, pinned[j["disp"]].data_ptr(), False)
-            for b in ("BLOCKS", "SBS", "COEFS", "CDEF_CHOICE") + (() if j["hidden"] else ("REC",)):
-                sess.lib.mav1cu_download(sess.h, mav1cu.BUF[b], out_bufs[b].data_ptr(), sizes[b])
-                d2h += sizes[b]
-        d2h_per_step = d2h
+            e2e_frame(g, j)
+
+    def d2h_bytes():
+        """Bytes one e2e step moves device->host, frame by frame (untimed)."""
+        total = 0
+        for g, j in order:
+            img = e2e_frame(g, j)
+            streams[g].synchronize()
+            h = img[:64].numpy().view(mav1cu.EXPORT_HEADER_DTYPE)[0]
+            assert h["status"] == 0
+            total += int(h["bytes"]) + (0 if j["hidden"] else geom["frame_bytes"])
+        return total
 
     def launches():
         return sum(st.launches() for st in streams)
@@ -194,6 +213,7 @@ def run_ours(args, rank, world):
         ms, nlaunch = timed(step_device, args.steps, args.warmup)
     ms_seq, _ = timed(step_sequential, max(1, args.steps // 2), 1)
     ms_e2e, _ = timed(step_e2e, max(1, args.steps // 2), 1)
+    d2h_per_step = d2h_bytes()
     per_step = sum(ms) / len(ms)
     per_e2e = sum(ms_e2e) / len(ms_e2e)
     per_seq = sum(ms_seq) / len(ms_seq)

@@ -292,6 +292,62 @@ int mav1cu_stream_join(mav1cu_stream *st, void *stream);
 /* Waits for every engine; returns the first sticky error. */
 int mav1cu_stream_synchronize(mav1cu_stream *st);
 
+/* ---- compact export of the writer inputs ---------------------------------
+ * No counterpart in the reference: its Metal backend shares full-size
+ * buffers with the host (unified memory). Here the entropy coder's inputs
+ * cross PCIe, so the device packs them into one image first:
+ *   superblock table  num_sbs records; first_block rewritten to the packed
+ *                     blocks (the only way the reference's host steps reach
+ *                     blocks: tile_writer.c:585, encoder.c:327-337,519,678,717)
+ *   CDEF choices      num_sbs int8
+ *   blocks            the num_blocks records in use, superblock order;
+ *                     coef_off[] rewritten into the level section
+ *   levels            a run of zero_run zeros, then, for every block that is
+ *                     not skipped, the levels of each plane with eob[plane]
+ *                     != 0 over its in-frame transform blocks (the region
+ *                     tile_writer.c:437-456 reads, ending with the last
+ *                     transform block's adjusted, at most 32 x 32, area);
+ *                     the other planes of such blocks point at the zero run
+ *                     (coef_off 0)
+ * Each section starts on a 256-byte boundary at the offset the header gives;
+ * the offsets depend on the frame size only. An image's sections read by
+ * the reference's writer as its BLOCKS / SBS / COEFS buffers give the same
+ * bitstream as the dense buffers. The image never needs more than
+ * mav1cu_export_capacity bytes: the level section is at most as long as
+ * the dense one. */
+typedef struct {
+  int32_t status;      /* 0 complete; 1 over capacity; 2 the session's blocks point outside its buffers
+                        * (1 and 2: nothing but the header is written) */
+  int32_t seq;         /* the session's export count, this export included */
+  int32_t num_sbs;     /* superblock table records */
+  int32_t num_blocks;  /* mav1cu_block_info records */
+  int32_t num_coefs;   /* int32 levels, the zero run included */
+  int32_t zero_run;    /* length of the leading run of zero levels */
+  int64_t sbs_off;     /* byte offsets of the sections from the start of the image */
+  int64_t cdef_off;
+  int64_t blocks_off;
+  int64_t coefs_off;
+  int64_t bytes;       /* bytes the export wrote: header and sections */
+} mav1cu_export_header;
+
+/* Bytes an export image of this session may need. */
+size_t mav1cu_export_capacity(const mav1cu_session *s);
+/* The session's own export image (page-locked host memory mapped into the
+ * device address space, mav1cu_export_capacity bytes), allocated on the first
+ * call and freed with the session; NULL (and a sticky error) if the
+ * allocation fails. */
+void *mav1cu_export_image(mav1cu_session *s);
+/* Enqueues, on the session's stream, the packing of the current frame's
+ * BLOCKS, SBS, COEFS and CDEF_CHOICE into `image`: page-locked host memory
+ * mapped into the device address space (cudaHostAlloc, cudaMallocHost or
+ * cudaHostRegister with mapping; the kernels store into it across the bus,
+ * so only the packed bytes travel and no copy size is needed up front) or
+ * memory of the session's device; 16-byte aligned, at least
+ * mav1cu_export_capacity bytes. The image is complete once the session's work
+ * so far has completed (mav1cu_synchronize, or an event recorded after this
+ * call); until then the caller must not read or reuse it. */
+int mav1cu_export(mav1cu_session *s, void *image, size_t cap);
+
 /* ---- host helpers (no device work) --------------------------------------- */
 /* Forward transform matrices (Q20), 15 x 4096 int32: least-squares inverses
  * of the normative inverse kernels. Replaces fwd_build_matrices

@@ -22,6 +22,7 @@
 #include "recon.cuh"
 #include "filters.cuh"
 #include "stream.cuh"
+#include "export.cuh"
 
 // dynamic shared memory of the analysis pass-1 kernel: a WarpMem per warp
 // and one reduction word per warp
@@ -78,6 +79,10 @@ struct mav1cu_session {
   int *blk_done;           // per-block completion flags of the recon launch: luma, then chroma
   int *dep_count, *succ_count, *succ, *queue, *qvalid;  // intra ready queue (rec::Ctx)
   int resident_recon;      // intra recon workers (CTAs, one per SM)
+  int4 *xcounts;           // compact export: per-superblock counts, block and level bases, zero run / fit flag
+  int *xblk_base, *xcoef_base, *xmeta;
+  void *ximage;            // session-owned export image (page-locked, mapped), allocated on first request
+  int xseq;                // exports enqueued
   std::vector<int> wave_start, wave_len;
   int wave_tile_w;
   FrameParams fp;          // host copy of the current parameters
@@ -236,9 +241,11 @@ static void free_all(mav1cu_session *s) {
   for (int i = 0; i < MAV1CU_BUF_COUNT; i++)
     if (s->buf[i]) cudaFree(s->buf[i]);
   void *extra[] = {s->qp[0], s->qp[1], s->dsrc, s->dref[0], s->dref[1], s->ys, s->uvs, s->waves, s->status, s->blk_at, s->blk_list,
-                   s->blk_done, s->mats_t, s->dep_count, s->succ_count, s->succ, s->queue, s->qvalid};
+                   s->blk_done, s->mats_t, s->dep_count, s->succ_count, s->succ, s->queue, s->qvalid,
+                   s->xcounts, s->xblk_base, s->xcoef_base, s->xmeta};
   for (void *p : extra)
     if (p) cudaFree(p);
+  if (s->ximage) cudaFreeHost(s->ximage);
   if (s->own_stream) cudaStreamDestroy(s->own_stream);
 }
 
@@ -294,6 +301,10 @@ extern "C" int mav1cu_session_create(int width, int height, int max_cdef_presets
   s->mats_dirty = 1;
   if (e == cudaSuccess) e = cudaMalloc(&s->blk_list, sizeof(int) * MAX_BLOCKS_PER_SB * nsb);
   if (e == cudaSuccess) e = cudaMalloc(&s->blk_done, 2 * sizeof(int) * MAX_BLOCKS_PER_SB * nsb);
+  if (e == cudaSuccess) e = cudaMalloc(&s->xcounts, sizeof(int4) * nsb);
+  if (e == cudaSuccess) e = cudaMalloc(&s->xblk_base, sizeof(int) * nsb);
+  if (e == cudaSuccess) e = cudaMalloc(&s->xcoef_base, sizeof(int) * nsb);
+  if (e == cudaSuccess) e = cudaMalloc(&s->xmeta, sizeof(int) * 4);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->own_stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) {
     snprintf(err, errlen, "device allocation failed: %s", cudaGetErrorString(e));
@@ -615,6 +626,69 @@ extern "C" int mav1cu_restore(mav1cu_session *s) {
                                                            U8(s, MAV1CU_BUF_LROUT),
                                                            (const LrUnit *)s->buf[MAV1CU_BUF_LRUNITS]);
   return after_launch(s, "loop restoration");
+}
+
+// ---- compact export of the writer inputs ------------------------------------------
+
+static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+// Section offsets of the export image; they depend on the geometry only.
+static xport::Header export_layout(const mav1cu_session *s) {
+  size_t nsb = (size_t)s->g.num_sbs;
+  xport::Header h = {};
+  h.num_sbs = (int32_t)nsb;
+  h.sbs_off = 256;
+  h.cdef_off = (int64_t)align256(h.sbs_off + nsb * sizeof(SbInfo));
+  h.blocks_off = (int64_t)align256(h.cdef_off + nsb);
+  h.coefs_off = (int64_t)align256(h.blocks_off + nsb * MAX_BLOCKS_PER_SB * sizeof(BlockInfo));
+  return h;
+}
+
+extern "C" size_t mav1cu_export_capacity(const mav1cu_session *s) {
+  return (size_t)export_layout(s).coefs_off + sizeof(int32_t) * COEFS_PER_SB * (size_t)s->g.num_sbs;
+}
+
+extern "C" void *mav1cu_export_image(mav1cu_session *s) {
+  if (s->err) return NULL;
+  if (!s->ximage && check_cuda(s, cudaHostAlloc(&s->ximage, mav1cu_export_capacity(s), cudaHostAllocMapped),
+                               "export image allocation")) {
+    s->ximage = NULL;
+    return NULL;
+  }
+  return s->ximage;
+}
+
+extern "C" int mav1cu_export(mav1cu_session *s, void *image, size_t cap) {
+  if (need_params(s)) return s->err;
+  size_t need = mav1cu_export_capacity(s);
+  if (!image || cap < need || ((uintptr_t)image & 15))
+    return set_error(s, MAV1CU_ERR_ARG, "export: image %p of %zu bytes (needs %zu bytes, 16-byte aligned)", image, cap,
+                     need);
+  cudaPointerAttributes a;
+  if (check_cuda(s, cudaPointerGetAttributes(&a, image), "export: image attributes")) return s->err;
+  uint8_t *dimg = NULL;
+  int dev = 0;
+  if (check_cuda(s, cudaGetDevice(&dev), "export: device")) return s->err;
+  if (a.type == cudaMemoryTypeHost) dimg = (uint8_t *)a.devicePointer;
+  else if ((a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged) && a.device == dev) dimg = (uint8_t *)image;
+  if (!dimg)
+    return set_error(s, MAV1CU_ERR_ARG,
+                     "export: image %p is neither mapped page-locked host memory nor memory of device %d", image, dev);
+  xport::Header layout = export_layout(s);
+  layout.seq = ++s->xseq;
+  size_t nsb = (size_t)s->g.num_sbs;
+  const BlockInfo *blocks = (const BlockInfo *)s->buf[MAV1CU_BUF_BLOCKS];
+  const SbInfo *sbs = (const SbInfo *)s->buf[MAV1CU_BUF_SBS];
+  xport::k_export_count<<<(unsigned)((nsb + 7) / 8), 256, 0, s->stream>>>(DP(s), blocks, sbs, (int)nsb, s->xcounts);
+  if (after_launch(s, "export count")) return s->err;
+  xport::k_export_scan<<<1, xport::SCAN_THREADS, 0, s->stream>>>(
+      s->xcounts, (int)nsb, s->xblk_base, s->xcoef_base, s->xmeta, (const int8_t *)s->buf[MAV1CU_BUF_CDEF_CHOICE],
+      dimg, layout, (long long)nsb * MAX_BLOCKS_PER_SB, (long long)nsb * COEFS_PER_SB);
+  if (after_launch(s, "export scan")) return s->err;
+  xport::k_export_write<<<(unsigned)nsb, xport::WRITE_THREADS, 0, s->stream>>>(
+      DP(s), blocks, sbs, (const int32_t *)s->buf[MAV1CU_BUF_COEFS], s->xblk_base, s->xcoef_base, s->xmeta, dimg,
+      layout);
+  return after_launch(s, "export write");
 }
 
 extern "C" int mav1cu_synchronize(mav1cu_session *s) {

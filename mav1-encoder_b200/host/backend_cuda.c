@@ -11,13 +11,18 @@
  * unchanged:
  *   motion_search  SRC REF GOLD          -> MVFIELD MVGOLD
  *   analyze        SRC REF GOLD MV*      -> BLOCKS SBS ACOSTS AINFOS
- *   recon          SRC REF GOLD BLOCKS SBS -> REC COEFS BLOCKS
- *   frame_core     SRC REF GOLD          -> MV* BLOCKS SBS COEFS REC (edge types on the device)
+ *   recon          SRC REF GOLD BLOCKS SBS -> REC, writer inputs
+ *   frame_core     SRC REF GOLD          -> MV* REC, writer inputs (edge types on the device)
  *   filter         REC LFMASK            -> REC CDEFBUF[0..n)
  *   restore        REC DBK LRUNITS LROUT -> LROUT
  * (the device copies of REC / COEFS are not initialised from the host:
  * recon writes every sample and coefficient the writer and the following
- * stages read).
+ * stages read). The writer inputs (BLOCKS, SBS, COEFS) come back as the
+ * device's compact export (mav1cu_export): only the blocks in use and the
+ * levels of coded planes cross the bus, into a page-locked image the
+ * session owns, and are copied into the encoder's buffers with first_block
+ * and coef_off rewritten, which every host step that follows reads them by
+ * (tile_writer.c:449,585, encoder.c:519-574).
  *
  * Selection: backend_cuda_create() is the factory; built with
  * -DMAV1_CUDA_AS_METAL it is also exported as backend_metal_create, so an
@@ -68,6 +73,33 @@ static void frame_inputs(CudaBackend *cb, struct Mav1Encoder *e) {
 
 static size_t bsize(CudaBackend *cb, int buf) { return mav1cu_buf_size(cb->s, buf); }
 
+static void export_writer_inputs(CudaBackend *cb) {
+  void *img = mav1cu_export_image(cb->s);
+  ok(cb, img ? mav1cu_export(cb->s, img, mav1cu_export_capacity(cb->s)) : MAV1CU_ERR_NOMEM);
+}
+
+static void section(CudaBackend *cb, Buf *dst, const mav1cu_export_header *h, int64_t off, size_t n) {
+  if (n > dst->size) {
+    ok(cb, MAV1CU_ERR_ARG);
+    return;
+  }
+  memcpy(dst->base, (const char *)h + off, n);
+}
+
+/* after the hook's synchronize: the image's sections into the encoder's buffers */
+static void unpack_writer_inputs(CudaBackend *cb, struct Mav1Encoder *e) {
+  const mav1cu_export_header *h = (const mav1cu_export_header *)mav1cu_export_image(cb->s);
+  if (cb->reported || !h) return;
+  if (h->status) {
+    fprintf(stderr, "mav1 cuda backend: export status %d\n", h->status);
+    cb->reported = 1;
+    return;
+  }
+  section(cb, &e->sbs, h, h->sbs_off, (size_t)h->num_sbs * sizeof(mav1cu_sb_info));
+  section(cb, &e->blocks, h, h->blocks_off, (size_t)h->num_blocks * sizeof(mav1cu_block_info));
+  section(cb, &e->coefs, h, h->coefs_off, (size_t)h->num_coefs * sizeof(int32_t));
+}
+
 static void cu_motion_search(Backend *b, struct Mav1Encoder *e) {
   CudaBackend *cb = (CudaBackend *)b;
   frame_inputs(cb, e);
@@ -97,9 +129,8 @@ static void cu_recon(Backend *b, struct Mav1Encoder *e) {
   put(cb, MAV1CU_BUF_SBS, &e->sbs);
   ok(cb, mav1cu_recon(cb->s));
   get(cb, MAV1CU_BUF_REC, &e->rec, e->frame_bytes);
-  get(cb, MAV1CU_BUF_COEFS, &e->coefs, bsize(cb, MAV1CU_BUF_COEFS));
-  get(cb, MAV1CU_BUF_BLOCKS, &e->blocks, bsize(cb, MAV1CU_BUF_BLOCKS));
-  ok(cb, mav1cu_synchronize(cb->s));
+  export_writer_inputs(cb);
+  if (ok(cb, mav1cu_synchronize(cb->s))) unpack_writer_inputs(cb, e);
 }
 
 static void cu_frame_core(Backend *b, struct Mav1Encoder *e) {
@@ -108,11 +139,9 @@ static void cu_frame_core(Backend *b, struct Mav1Encoder *e) {
   ok(cb, mav1cu_frame_core(cb->s));
   get(cb, MAV1CU_BUF_MVFIELD, &e->mvfield, bsize(cb, MAV1CU_BUF_MVFIELD));
   get(cb, MAV1CU_BUF_MVGOLD, &e->mvgold, bsize(cb, MAV1CU_BUF_MVGOLD));
-  get(cb, MAV1CU_BUF_BLOCKS, &e->blocks, bsize(cb, MAV1CU_BUF_BLOCKS));
-  get(cb, MAV1CU_BUF_SBS, &e->sbs, bsize(cb, MAV1CU_BUF_SBS));
-  get(cb, MAV1CU_BUF_COEFS, &e->coefs, bsize(cb, MAV1CU_BUF_COEFS));
   get(cb, MAV1CU_BUF_REC, &e->rec, e->frame_bytes);
-  ok(cb, mav1cu_synchronize(cb->s));
+  export_writer_inputs(cb);
+  if (ok(cb, mav1cu_synchronize(cb->s))) unpack_writer_inputs(cb, e);
 }
 
 static void cu_filter(Backend *b, struct Mav1Encoder *e) {

@@ -53,7 +53,11 @@ JOB_DTYPE = np.dtype([(n, "<i4") for n in [
     "disp", "is_key", "kind", "last_slot", "arf_slot", "refresh", "hidden", "base_q_idx", "order_hint", "nonref",
     "leafopt", "reference_select", "golden_refresh", "gold_differs", "show_existing", "pad"]])
 assert PARAMS_DTYPE.itemsize == 392 and BLOCK_DTYPE.itemsize == 108
-assert SB_DTYPE.itemsize == 356 and LRUNIT_DTYPE.itemsize == 48
+EXPORT_HEADER_DTYPE = np.dtype([
+    ("status", "<i4"), ("seq", "<i4"), ("num_sbs", "<i4"), ("num_blocks", "<i4"), ("num_coefs", "<i4"),
+    ("zero_run", "<i4"), ("sbs_off", "<i8"), ("cdef_off", "<i8"), ("blocks_off", "<i8"), ("coefs_off", "<i8"),
+    ("bytes", "<i8")])
+assert SB_DTYPE.itemsize == 356 and LRUNIT_DTYPE.itemsize == 48 and EXPORT_HEADER_DTYPE.itemsize == 64
 
 EXPORTS = [
     "mav1cu_session_create", "mav1cu_session_destroy", "mav1cu_set_stream", "mav1cu_get_stream", "mav1cu_buf_size",
@@ -64,6 +68,7 @@ EXPORTS = [
     "mav1cu_frame_params_for", "mav1cu_stream_create", "mav1cu_stream_destroy", "mav1cu_stream_session",
     "mav1cu_stream_encode", "mav1cu_stream_slot", "mav1cu_stream_engines", "mav1cu_stream_engine",
     "mav1cu_stream_wait", "mav1cu_stream_join", "mav1cu_stream_synchronize", "mav1cu_edge_types_noalloc",
+    "mav1cu_export_capacity", "mav1cu_export_image", "mav1cu_export",
 ]
 
 
@@ -126,6 +131,12 @@ def load_library(path=LIB_PATH):
     lib.mav1cu_stream_synchronize.restype = i32
     lib.mav1cu_edge_types_noalloc.argtypes = [vp, vp, vp, i32, i32, i32, vp, ctypes.c_char_p, sz]
     lib.mav1cu_edge_types_noalloc.restype = i32
+    lib.mav1cu_export_capacity.argtypes = [vp]
+    lib.mav1cu_export_capacity.restype = sz
+    lib.mav1cu_export_image.argtypes = [vp]
+    lib.mav1cu_export_image.restype = vp
+    lib.mav1cu_export.argtypes = [vp, vp, sz]
+    lib.mav1cu_export.restype = i32
     return lib
 
 
@@ -249,8 +260,38 @@ class Session:
     def synchronize(self):
         self._check(self.lib.mav1cu_synchronize(self.h), "synchronize")
 
+    def export_capacity(self):
+        return self.lib.mav1cu_export_capacity(self.h)
+
+    def export(self, image_ptr=None, cap=None):
+        """Enqueues the compact export of the writer inputs into image_ptr
+        (mapped page-locked host or device memory), or into the session's own
+        image; returns the image's address."""
+        if image_ptr is None:
+            image_ptr = self.lib.mav1cu_export_image(self.h)
+            if not image_ptr:
+                self._check(-2, "export image")
+        cap = self.export_capacity() if cap is None else cap
+        self._check(self.lib.mav1cu_export(self.h, image_ptr, cap), "export")
+        return image_ptr
+
     def launches(self):
         return self.lib.mav1cu_launch_count(self.h)
+
+
+def export_sections(image):
+    """(header, superblocks, CDEF choices, blocks, levels) of an export image
+    held in a uint8 array."""
+    h = image[:EXPORT_HEADER_DTYPE.itemsize].view(EXPORT_HEADER_DTYPE)[0]
+    if h["status"]:
+        raise Mav1cuError(f"export image status {int(h['status'])}")
+    nsb, nb, nc = int(h["num_sbs"]), int(h["num_blocks"]), int(h["num_coefs"])
+
+    def sect(off, dtype, n):
+        return image[int(off):int(off) + n * np.dtype(dtype).itemsize].view(dtype)
+
+    return (h, sect(h["sbs_off"], SB_DTYPE, nsb), sect(h["cdef_off"], np.int8, nsb),
+            sect(h["blocks_off"], BLOCK_DTYPE, nb), sect(h["coefs_off"], np.int32, nc))
 
 
 def cli_config(width, height, q=100, keyint=0, lf=1, cdef=1, txs=1, txd=1, lr=1, lr_test=0, sw=1, fast=0, turbo=0,

@@ -376,3 +376,69 @@ def stream_vs_oracle(tr, frames, flags, spec):
     finally:
         st.close()
     return res
+
+
+# ---- compact export of the writer inputs ------------------------------------------
+
+
+def pack_writer_inputs(blocks, sbs, coefs, cdef, p):
+    """The compact export image's sections (mav1cu_export) restated from the
+    dense BLOCKS / SBS / COEFS / CDEF_CHOICE buffers: the blocks in use with
+    first_block and coef_off rewritten, and a level run that opens with
+    zeros as long as the largest zero plane of a coded block, followed by
+    the levels of every coded plane (eob != 0) of every coded block over the
+    transform blocks the writer visits (tile_writer.c:437-456), up to the
+    last level it may read."""
+    T = spec_tables()
+
+    def region(b, plane):
+        # transform blocks tw * th apart; the writer reads the last one only
+        # inside its adjusted (at most 32 x 32) transform
+        tx, starts = tx_layout(b, plane, p)
+        w, h = int(T["Tx_Width"][tx]), int(T["Tx_Height"][tx])
+        return (len(starts) - 1) * w * h + min(32, w) * min(32, h) if starts else 0
+
+    used = [blocks[r["first_block"]: r["first_block"] + r["num_blocks"]] for r in sbs]
+    zrun = 0
+    for bl in used:
+        for b in bl:
+            if b["eob"].any():
+                zrun = max([zrun] + [region(b, pl) for pl in range(3) if not b["eob"][pl]])
+    out_sbs = sbs.copy()
+    out_blocks = np.concatenate(used).copy() if used else np.zeros(0, BLOCK_DTYPE)
+    levels = [np.zeros(zrun, np.int32)]
+    pos, k = zrun, 0
+    for i, bl in enumerate(used):
+        out_sbs[i]["first_block"] = k
+        for b in bl:
+            nb = out_blocks[k]
+            for pl in range(3):
+                if b["eob"].any() and b["eob"][pl]:
+                    n = region(b, pl)
+                    o = int(b["coef_off"][pl])
+                    levels.append(np.asarray(coefs[o: o + n], np.int32))
+                    nb["coef_off"][pl] = pos
+                    pos += n
+                else:
+                    nb["coef_off"][pl] = 0
+            k += 1
+    return dict(sbs=out_sbs, cdef=np.asarray(cdef[: len(sbs)], np.int8), blocks=out_blocks,
+                levels=np.concatenate(levels), zero_run=zrun)
+
+
+def export_vs_packed(image, blocks, sbs, coefs, cdef, p):
+    """Mismatch counts between an export image (uint8 array) and the packing
+    of the dense buffers it was made from."""
+    h, isbs, icdef, iblocks, ilevels = mav1cu.export_sections(image)
+    want = pack_writer_inputs(blocks, sbs, coefs, cdef, p)
+    out = dict(zero_run=int(h["zero_run"] != want["zero_run"]),
+               num_blocks=int(h["num_blocks"] != len(want["blocks"])),
+               num_coefs=int(h["num_coefs"] != len(want["levels"])))
+    out["sbs"] = int((isbs != want["sbs"]).sum()) if len(isbs) == len(want["sbs"]) else -1
+    out["cdef"] = int((icdef != want["cdef"]).sum())
+    out["blocks"] = int((iblocks != want["blocks"]).sum()) if len(iblocks) == len(want["blocks"]) else -1
+    out["levels"] = int((ilevels != want["levels"]).sum()) if len(ilevels) == len(want["levels"]) else -1
+    nbytes = (64 + len(isbs) * SB_DTYPE.itemsize + len(icdef) + len(iblocks) * BLOCK_DTYPE.itemsize +
+              4 * len(ilevels))
+    out["bytes"] = int(h["bytes"] != nbytes)
+    return out
