@@ -15,13 +15,14 @@ not part of this path) are not timed.
 value: frames/s with the source frames resident in HBM (CUDA events on the
        session stream, max over ranks).
 e2e:   the same through the C ABI from pinned host memory: every frame's
-       source is copied host->device, its entropy-coder inputs (superblock
-       table, CDEF choices, the blocks in use, the levels of coded planes)
-       are packed on the device and stored into mapped pinned host memory
-       (mav1cu_export), and the shown frames' reconstructions are copied
-       device->host, all inside the timed region. d2h_bytes_per_step counts
-       the bytes each frame's export image holds (its header's byte count,
-       read in an untimed pass over the same step) plus the reconstructions.
+       source is copied host->device (an upload stream per engine, ahead of
+       the engine), and its entropy-coder inputs (superblock table, CDEF
+       choices, the blocks in use, the levels of coded planes) plus, for
+       shown frames, the visible I420 reconstruction are packed on the device
+       and stored into mapped pinned host memory (mav1cu_export, on each
+       engine's transfer stream), all inside the timed region.
+       d2h_bytes_per_step counts the bytes the export images hold (their
+       headers' byte counts, read in an untimed pass over the same step).
 --impl reference: the reference encoder's own scalar CPU path (oracle/_ref,
        built from the reference sources) on the host cores, all threads.
 
@@ -137,7 +138,6 @@ def run_ours(args, rank, world):
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{dev}")
     pinned = torch.from_numpy(frames_host).pin_memory()
     geom = mav1cu.geometry(SPEC.width, SPEC.height)
-    rec_out = torch.empty(geom["frame_bytes"], dtype=torch.uint8).pin_memory()
     # one export image per engine of each GOP stream: a frame's image stays
     # intact until that engine's next frame
     cap = streams[0].session.export_capacity()
@@ -154,9 +154,7 @@ def run_ours(args, rank, world):
     def e2e_frame(g, j):
         sess = streams[g].encode(j, pinned[j["disp"]].data_ptr(), False)
         img = images[(g, mav1cu.Stream.engine_of(j))]
-        sess.export(img.data_ptr(), cap)
-        if not j["hidden"]:
-            sess.lib.mav1cu_download(sess.h, mav1cu.BUF["REC"], rec_out.data_ptr(), geom["frame_bytes"])
+        sess.export(img.data_ptr(), cap, rec=not j["hidden"])
         return img
 
     def step_e2e():
@@ -169,9 +167,9 @@ def run_ours(args, rank, world):
         for g, j in order:
             img = e2e_frame(g, j)
             streams[g].synchronize()
-            h = img[:64].numpy().view(mav1cu.EXPORT_HEADER_DTYPE)[0]
+            h = img[:mav1cu.EXPORT_HEADER_DTYPE.itemsize].numpy().view(mav1cu.EXPORT_HEADER_DTYPE)[0]
             assert h["status"] == 0
-            total += int(h["bytes"]) + (0 if j["hidden"] else geom["frame_bytes"])
+            total += int(h["bytes"])
         return total
 
     def launches():

@@ -309,6 +309,11 @@ int mav1cu_stream_synchronize(mav1cu_stream *st);
  *                     transform block's adjusted, at most 32 x 32, area);
  *                     the other planes of such blocks point at the zero run
  *                     (coef_off 0)
+ *   reconstruction    (MAV1CU_EXPORT_REC) the shown picture as
+ *                     mav1_get_recon returns it (encoder.c:877-915): the
+ *                     visible width x height luma samples, then each
+ *                     chroma plane's (width+1)/2 x (height+1)/2 samples,
+ *                     rows packed
  * Each section starts on a 256-byte boundary at the offset the header gives;
  * the offsets depend on the frame size only. An image's sections read by
  * the reference's writer as its BLOCKS / SBS / COEFS buffers give the same
@@ -327,8 +332,12 @@ typedef struct {
   int64_t cdef_off;
   int64_t blocks_off;
   int64_t coefs_off;
+  int64_t rec_off;
+  int64_t rec_bytes;   /* bytes of the reconstruction section (0 without MAV1CU_EXPORT_REC) */
   int64_t bytes;       /* bytes the export wrote: header and sections */
 } mav1cu_export_header;
+
+enum { MAV1CU_EXPORT_REC = 1 };
 
 /* Bytes an export image of this session may need. */
 size_t mav1cu_export_capacity(const mav1cu_session *s);
@@ -337,16 +346,21 @@ size_t mav1cu_export_capacity(const mav1cu_session *s);
  * call and freed with the session; NULL (and a sticky error) if the
  * allocation fails. */
 void *mav1cu_export_image(mav1cu_session *s);
-/* Enqueues, on the session's stream, the packing of the current frame's
- * BLOCKS, SBS, COEFS and CDEF_CHOICE into `image`: page-locked host memory
- * mapped into the device address space (cudaHostAlloc, cudaMallocHost or
- * cudaHostRegister with mapping; the kernels store into it across the bus,
- * so only the packed bytes travel and no copy size is needed up front) or
- * memory of the session's device; 16-byte aligned, at least
- * mav1cu_export_capacity bytes. The image is complete once the session's work
- * so far has completed (mav1cu_synchronize, or an event recorded after this
- * call); until then the caller must not read or reuse it. */
-int mav1cu_export(mav1cu_session *s, void *image, size_t cap);
+/* Enqueues the packing of the current frame's BLOCKS, SBS, COEFS and
+ * CDEF_CHOICE (and with MAV1CU_EXPORT_REC in flags its REC) into `image`:
+ * page-locked host memory mapped into the device address space
+ * (cudaHostAlloc, cudaMallocHost or cudaHostRegister with mapping; the
+ * kernels store into it across the bus, so only the packed bytes travel and
+ * no copy size is needed up front) or memory of the session's device;
+ * 16-byte aligned, at least mav1cu_export_capacity bytes.
+ * The packing runs on the session's transfer stream, after the work enqueued
+ * on the session's stream so far; the session's next stage that rewrites one
+ * of those buffers (analysis, edge types, recon, filter, CDEF selection, an
+ * upload or copy) waits for it, and motion search, which does not, overlaps
+ * it. The image is complete after mav1cu_synchronize (or, for a stream,
+ * mav1cu_stream_synchronize / mav1cu_stream_join, which cover the transfer
+ * streams); until then the caller must not read or reuse it. */
+int mav1cu_export(mav1cu_session *s, void *image, size_t cap, int flags);
 
 /* ---- host helpers (no device work) --------------------------------------- */
 /* Forward transform matrices (Q20), 15 x 4096 int32: least-squares inverses

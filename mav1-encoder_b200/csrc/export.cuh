@@ -30,12 +30,26 @@ constexpr int SB_WORDS = (int)(sizeof(SbInfo) / 4);
 constexpr int BLK_WORDS = (int)(sizeof(BlockInfo) / 4);
 constexpr int WRITE_THREADS = 128;
 constexpr int SCAN_THREADS = 1024;
+// CTAs of the kernels that store into the image: the stores are paced by the
+// bus, and a small persistent grid leaves the other SMs (and their shared
+// memory) to the frame engines the export overlaps
+#ifndef MAV1CU_STORE_CTAS
+#define MAV1CU_STORE_CTAS 16
+#endif
+constexpr int STORE_CTAS = MAV1CU_STORE_CTAS;
 
 struct Header {  // mav1cu_export_header
   int32_t status, seq, num_sbs, num_blocks, num_coefs, zero_run;
-  int64_t sbs_off, cdef_off, blocks_off, coefs_off, bytes;
+  int64_t sbs_off, cdef_off, blocks_off, coefs_off, rec_off, rec_bytes, bytes;
 };
-static_assert(sizeof(Header) == 64, "export header layout");
+static_assert(sizeof(Header) == 80, "export header layout");
+
+// The frame parameters the packing depends on, passed by value: the export
+// runs on its own stream and must not read PARAMS, which the next frame's
+// set-up rewrites.
+struct Frame {
+  int mi_cols, mi_rows, lossless;
+};
 
 // Levels of `plane` of block b that the writer may read: the plane's
 // transform blocks whose start lies inside the frame, tw * th apart
@@ -44,15 +58,15 @@ static_assert(sizeof(Header) == 64, "export header layout");
 // (find_eob, k_recon.h:50-54; write_coeffs, tile_writer.c:177-178,228-229),
 // which lie inside the adjusted transform (at most 32 x 32, the first
 // min(32, tw) * min(32, th) levels), so the run ends there.
-HD int plane_levels(const FrameParams *fp, const BlockInfo &b, int plane) {
+HD int plane_levels(const Frame &f, const BlockInfo &b, int plane) {
   int bs = b.bsize, sub = plane > 0;
-  int txSz = fp->lossless ? TX_4X4
+  int txSz = f.lossless ? TX_4X4
              : plane == 0 ? (b.is_inter ? T(Max_Tx_Size_Rect)[bs] : depth_tx_size(bs, b.tx_depth))
                           : uv_tx_size(bs, 1, 1);
   int tw = T(Tx_Width)[txSz], th = T(Tx_Height)[txSz];
   int psz = T(Subsampled_Size)[bs][sub][sub];
   int pw = block_w(psz), ph = block_h(psz);
-  int maxX = (fp->mi_cols * 4) >> sub, maxY = (fp->mi_rows * 4) >> sub;
+  int maxX = (f.mi_cols * 4) >> sub, maxY = (f.mi_rows * 4) >> sub;
   int x0 = (b.mi_col >> sub) * 4, y0 = (b.mi_row >> sub) * 4;
   int nx = imin((pw + tw - 1) / tw, (imax(0, maxX - x0) + tw - 1) / tw);
   int ny = imin((ph + th - 1) / th, (imax(0, maxY - y0) + th - 1) / th);
@@ -66,8 +80,7 @@ HD int block_skipped(const BlockInfo &b) { return b.eob[0] == 0 && b.eob[1] == 0
 // .w when its table entry or blocks point outside the session's buffers (the
 // write kernel reads only ranges checked here). One warp per superblock,
 // lanes over its blocks.
-__global__ void k_export_count(const FrameParams *fp, const BlockInfo *blocks, const SbInfo *sbs, int num_sbs,
-                               int4 *counts) {
+__global__ void k_export_count(Frame f, const BlockInfo *blocks, const SbInfo *sbs, int num_sbs, int4 *counts) {
   int sb = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
   if (sb >= num_sbs) return;
   long long nblk = (long long)num_sbs * MAX_BLOCKS_PER_SB, ncoef = (long long)num_sbs * COEFS_PER_SB;
@@ -83,7 +96,7 @@ __global__ void k_export_count(const FrameParams *fp, const BlockInfo *blocks, c
       continue;
     }
     for (int p = 0; p < 3; p++) {
-      int n = plane_levels(fp, b, p);
+      int n = plane_levels(f, b, p);
       if (b.eob[p]) {
         coded += n;
         bad |= b.coef_off[p] < 0 || (b.coef_off[p] & 3) || (long long)b.coef_off[p] + n > ncoef;
@@ -195,23 +208,19 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_export_scan(const int4 *counts
     h.num_coefs = (int32_t)ncoefs;
     h.zero_run = zrun;
     h.bytes = fits ? (long long)sizeof(Header) + (long long)num_sbs * (SB_WORDS * 4 + 1) + nblocks * BLK_WORDS * 4 +
-                         ncoefs * 4
+                         ncoefs * 4 + layout.rec_bytes
                    : (long long)sizeof(Header);
+    if (!fits) h.rec_bytes = 0;
     *(Header *)image = h;
   }
 }
 
-// One CTA per superblock: its table entry, its blocks with coef_off
-// rewritten, and the levels of its coded planes.
-__global__ void __launch_bounds__(WRITE_THREADS) k_export_write(const FrameParams *fp, const BlockInfo *blocks,
-                                                                 const SbInfo *sbs, const int32_t *coefs,
-                                                                 const int *blk_base, const int *coef_base,
-                                                                 const int *meta, uint8_t *image, Header layout) {
-  __shared__ BlockInfo sblk[MAX_BLOCKS_PER_SB];
-  __shared__ int rel4[3 * MAX_BLOCKS_PER_SB], src4[3 * MAX_BLOCKS_PER_SB];
-  __shared__ int wtot[WRITE_THREADS / 32];
-  if (!meta[1]) return;
-  int sb = blockIdx.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+// One superblock: its table entry, its blocks with coef_off rewritten, and
+// the levels of its coded planes. Shared state: the CTA's.
+__device__ void write_sb(const Frame &f, const BlockInfo *blocks, const SbInfo *sbs, int sb, const int32_t *coefs,
+                         const int *blk_base, const int *coef_base, const int *meta, uint8_t *image,
+                         const Header &layout, BlockInfo *sblk, int *rel4, int *src4, int *wtot) {
+  int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const SbInfo &s = sbs[sb];
   int nb = imin(s.num_blocks, MAX_BLOCKS_PER_SB), first = s.first_block, bb = blk_base[sb];
   int zrun = meta[0], cbase = zrun + coef_base[sb];
@@ -225,7 +234,7 @@ __global__ void __launch_bounds__(WRITE_THREADS) k_export_write(const FrameParam
   int n[3] = {0, 0, 0};
   if (tid < nb && !block_skipped(sblk[tid]))
     for (int p = 0; p < 3; p++)
-      if (sblk[tid].eob[p]) n[p] = plane_levels(fp, sblk[tid], p);
+      if (sblk[tid].eob[p]) n[p] = plane_levels(f, sblk[tid], p);
   int tot = n[0] + n[1] + n[2], x = tot;
   for (int o = 1; o < 32; o <<= 1) {
     int t = __shfl_up_sync(0xffffffffu, x, o);
@@ -263,6 +272,43 @@ __global__ void __launch_bounds__(WRITE_THREADS) k_export_write(const FrameParam
       else hi = mid - 1;
     }
     d4[i] = __ldcs(c4 + src4[lo] + (i - rel4[lo]));
+  }
+}
+
+// STORE_CTAS CTAs, striding over the superblocks.
+__global__ void __launch_bounds__(WRITE_THREADS) k_export_write(Frame f, const BlockInfo *blocks, const SbInfo *sbs,
+                                                                 int num_sbs, const int32_t *coefs,
+                                                                 const int *blk_base, const int *coef_base,
+                                                                 const int *meta, uint8_t *image, Header layout) {
+  __shared__ BlockInfo sblk[MAX_BLOCKS_PER_SB];
+  __shared__ int rel4[3 * MAX_BLOCKS_PER_SB], src4[3 * MAX_BLOCKS_PER_SB];
+  __shared__ int wtot[WRITE_THREADS / 32];
+  if (!meta[1]) return;
+  for (int sb = blockIdx.x; sb < num_sbs; sb += gridDim.x) {
+    write_sb(f, blocks, sbs, sb, coefs, blk_base, coef_base, meta, image, layout, sblk, rel4, src4, wtot);
+    __syncthreads();  // this superblock's shared state is consumed
+  }
+}
+
+// The shown reconstruction as mav1_get_recon returns it (encoder.c:877-915):
+// the visible w x h luma samples, then the (w+1)/2 x (h+1)/2 samples of each
+// chroma plane, rows packed. STORE_CTAS CTAs stride over the output rows;
+// 16-byte stores where the row width and both row starts allow.
+__global__ void k_export_rec(const uint8_t *rec, int3 offset, int2 stride, int w, int h, const int *meta,
+                             uint8_t *dst) {
+  if (!meta[1]) return;
+  int cw = (w + 1) >> 1, ch = (h + 1) >> 1;
+  for (int row = blockIdx.x; row < h + 2 * ch; row += gridDim.x) {
+    int p = row < h ? 0 : row < h + ch ? 1 : 2;
+    int r = p == 0 ? row : p == 1 ? row - h : row - h - ch;
+    int pw = p ? cw : w;
+    const uint8_t *s = rec + (p == 0 ? offset.x : p == 1 ? offset.y : offset.z) + (size_t)r * (p ? stride.y : stride.x);
+    uint8_t *d = dst + (p == 0 ? (size_t)r * w : (size_t)w * h + (size_t)(p - 1) * cw * ch + (size_t)r * cw);
+    if (!(pw & 15) && !((uintptr_t)s & 15) && !((uintptr_t)d & 15)) {
+      for (int k = threadIdx.x; k < pw / 16; k += blockDim.x) ((int4 *)d)[k] = __ldcs((const int4 *)s + k);
+    } else {
+      for (int k = threadIdx.x; k < pw; k += blockDim.x) d[k] = s[k];
+    }
   }
 }
 

@@ -83,6 +83,9 @@ struct mav1cu_session {
   int *xblk_base, *xcoef_base, *xmeta;
   void *ximage;            // session-owned export image (page-locked, mapped), allocated on first request
   int xseq;                // exports enqueued
+  cudaStream_t xs;         // transfer stream the exports run on, forked from `stream`
+  cudaEvent_t x_fork, x_done;
+  int x_pending;           // an export may still read the session's buffers: writers wait for x_done
   std::vector<int> wave_start, wave_len;
   int wave_tile_w;
   FrameParams fp;          // host copy of the current parameters
@@ -111,6 +114,15 @@ static int check_cuda(mav1cu_session *s, cudaError_t e, const char *what) {
 static int after_launch(mav1cu_session *s, const char *what) {
   s->launches++;
   return check_cuda(s, cudaGetLastError(), what);
+}
+
+// Work that overwrites an exported buffer (BLOCKS, SBS, COEFS, CDEF_CHOICE,
+// REC) waits until the export reading it, on the transfer stream, is done.
+static void export_fence(mav1cu_session *s) {
+  if (s->x_pending) {
+    cudaStreamWaitEvent(s->stream, s->x_done, 0);
+    s->x_pending = 0;
+  }
 }
 
 // ---- inverse scan tables ------------------------------------------------------------
@@ -246,6 +258,9 @@ static void free_all(mav1cu_session *s) {
   for (void *p : extra)
     if (p) cudaFree(p);
   if (s->ximage) cudaFreeHost(s->ximage);
+  if (s->x_fork) cudaEventDestroy(s->x_fork);
+  if (s->x_done) cudaEventDestroy(s->x_done);
+  if (s->xs) cudaStreamDestroy(s->xs);
   if (s->own_stream) cudaStreamDestroy(s->own_stream);
 }
 
@@ -306,6 +321,9 @@ extern "C" int mav1cu_session_create(int width, int height, int max_cdef_presets
   if (e == cudaSuccess) e = cudaMalloc(&s->xcoef_base, sizeof(int) * nsb);
   if (e == cudaSuccess) e = cudaMalloc(&s->xmeta, sizeof(int) * 4);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->own_stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->xs, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->x_fork, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->x_done, cudaEventDisableTiming);
   if (e != cudaSuccess) {
     snprintf(err, errlen, "device allocation failed: %s", cudaGetErrorString(e));
     free_all(s);
@@ -343,6 +361,7 @@ extern "C" int mav1cu_session_create(int width, int height, int max_cdef_presets
 extern "C" void mav1cu_session_destroy(mav1cu_session *s) {
   if (!s) return;
   cudaStreamSynchronize(s->stream);
+  if (s->xs) cudaStreamSynchronize(s->xs);
   free_all(s);
   delete s;
 }
@@ -366,6 +385,7 @@ extern "C" int mav1cu_upload(mav1cu_session *s, int buf, const void *host, size_
   if (buf < 0 || buf >= MAV1CU_BUF_COUNT || bytes > s->size[buf])
     return set_error(s, MAV1CU_ERR_ARG, "upload: buffer %d, %zu bytes", buf, bytes);
   if (buf == MAV1CU_BUF_MATS) s->mats_dirty = 1;
+  export_fence(s);
   return check_cuda(s, cudaMemcpyAsync(s->buf[buf], host, bytes, cudaMemcpyHostToDevice, s->stream), "upload");
 }
 
@@ -381,6 +401,7 @@ extern "C" int mav1cu_copy(mav1cu_session *s, int dst, int src, size_t bytes) {
   if (dst < 0 || dst >= MAV1CU_BUF_COUNT || src < 0 || src >= MAV1CU_BUF_COUNT || bytes > s->size[dst] ||
       bytes > s->size[src])
     return set_error(s, MAV1CU_ERR_ARG, "copy: buffers %d <- %d, %zu bytes", dst, src, bytes);
+  export_fence(s);
   if (dst == MAV1CU_BUF_MATS) s->mats_dirty = 1;
   return check_cuda(s, cudaMemcpyAsync(s->buf[dst], s->buf[src], bytes, cudaMemcpyDeviceToDevice, s->stream), "copy");
 }
@@ -489,6 +510,7 @@ static ana::Ctx ana_ctx(mav1cu_session *s) {
 
 extern "C" int mav1cu_analyze(mav1cu_session *s) {
   if (need_params(s)) return s->err;
+  export_fence(s);
   ana::Ctx c = ana_ctx(s);
   for (int level = 0; level < 4; level++) {
     int slots = ana::level_slots(&s->fp, level);
@@ -504,6 +526,7 @@ extern "C" int mav1cu_analyze(mav1cu_session *s) {
 
 extern "C" int mav1cu_edge_types(mav1cu_session *s) {
   if (need_params(s)) return s->err;
+  export_fence(s);
   BlockInfo *blocks = (BlockInfo *)s->buf[MAV1CU_BUF_BLOCKS];
   const SbInfo *sbs = (const SbInfo *)s->buf[MAV1CU_BUF_SBS];
   ana::k_edge_marks<<<s->g.num_sbs, 64, 0, s->stream>>>(DP(s), blocks, sbs, s->ys, s->uvs);
@@ -514,6 +537,7 @@ extern "C" int mav1cu_edge_types(mav1cu_session *s) {
 
 extern "C" int mav1cu_recon(mav1cu_session *s) {
   if (need_params(s)) return s->err;
+  export_fence(s);
   rec::Ctx c;
   c.fp = DP(s);
   c.src = U8(s, MAV1CU_BUF_SRC);
@@ -590,6 +614,7 @@ extern "C" int mav1cu_filter(mav1cu_session *s, int num_cdef_presets) {
   if (need_params(s)) return s->err;
   if (num_cdef_presets < 0 || num_cdef_presets > s->max_presets)
     return set_error(s, MAV1CU_ERR_ARG, "filter: %d CDEF presets (session holds %d)", num_cdef_presets, s->max_presets);
+  export_fence(s);
   const FrameParams &fp = s->fp;
   if (fp.lf_level[0] || fp.lf_level[1] || fp.lf_level[2] || fp.lf_level[3]) {
     for (int pass = 0; pass < 2; pass++) {
@@ -613,6 +638,7 @@ extern "C" int mav1cu_cdef_select(mav1cu_session *s, int num_cdef_presets) {
   if (need_params(s)) return s->err;
   if (num_cdef_presets < 1 || num_cdef_presets > s->max_presets)
     return set_error(s, MAV1CU_ERR_ARG, "cdef_select: %d presets (session holds %d)", num_cdef_presets, s->max_presets);
+  export_fence(s);
   flt::k_cdef_select<<<s->g.num_sbs, 256, 0, s->stream>>>(DP(s), U8(s, MAV1CU_BUF_SRC), U8(s, MAV1CU_BUF_CDEFBUF),
                                                            (long long)s->g.frame_bytes, U8(s, MAV1CU_BUF_REC),
                                                            (int8_t *)s->buf[MAV1CU_BUF_CDEF_CHOICE], num_cdef_presets);
@@ -641,11 +667,17 @@ static xport::Header export_layout(const mav1cu_session *s) {
   h.cdef_off = (int64_t)align256(h.sbs_off + nsb * sizeof(SbInfo));
   h.blocks_off = (int64_t)align256(h.cdef_off + nsb);
   h.coefs_off = (int64_t)align256(h.blocks_off + nsb * MAX_BLOCKS_PER_SB * sizeof(BlockInfo));
+  h.rec_off = (int64_t)align256(h.coefs_off + sizeof(int32_t) * COEFS_PER_SB * nsb);
   return h;
 }
 
+// Bytes of the visible I420 picture (mav1_get_recon's planes).
+static size_t i420_bytes(const Geometry &g) {
+  return (size_t)g.w * g.h + 2 * (size_t)((g.w + 1) >> 1) * ((g.h + 1) >> 1);
+}
+
 extern "C" size_t mav1cu_export_capacity(const mav1cu_session *s) {
-  return (size_t)export_layout(s).coefs_off + sizeof(int32_t) * COEFS_PER_SB * (size_t)s->g.num_sbs;
+  return (size_t)export_layout(s).rec_off + i420_bytes(s->g);
 }
 
 extern "C" void *mav1cu_export_image(mav1cu_session *s) {
@@ -658,8 +690,9 @@ extern "C" void *mav1cu_export_image(mav1cu_session *s) {
   return s->ximage;
 }
 
-extern "C" int mav1cu_export(mav1cu_session *s, void *image, size_t cap) {
+extern "C" int mav1cu_export(mav1cu_session *s, void *image, size_t cap, int flags) {
   if (need_params(s)) return s->err;
+  if (flags & ~MAV1CU_EXPORT_REC) return set_error(s, MAV1CU_ERR_ARG, "export: unknown flags 0x%x", flags);
   size_t need = mav1cu_export_capacity(s);
   if (!image || cap < need || ((uintptr_t)image & 15))
     return set_error(s, MAV1CU_ERR_ARG, "export: image %p of %zu bytes (needs %zu bytes, 16-byte aligned)", image, cap,
@@ -676,24 +709,45 @@ extern "C" int mav1cu_export(mav1cu_session *s, void *image, size_t cap) {
                      "export: image %p is neither mapped page-locked host memory nor memory of device %d", image, dev);
   xport::Header layout = export_layout(s);
   layout.seq = ++s->xseq;
+  int withRec = flags & MAV1CU_EXPORT_REC;
+  layout.rec_bytes = withRec ? (int64_t)i420_bytes(s->g) : 0;
   size_t nsb = (size_t)s->g.num_sbs;
   const BlockInfo *blocks = (const BlockInfo *)s->buf[MAV1CU_BUF_BLOCKS];
   const SbInfo *sbs = (const SbInfo *)s->buf[MAV1CU_BUF_SBS];
-  xport::k_export_count<<<(unsigned)((nsb + 7) / 8), 256, 0, s->stream>>>(DP(s), blocks, sbs, (int)nsb, s->xcounts);
+  xport::Frame f = {s->fp.mi_cols, s->fp.mi_rows, s->fp.lossless};
+  // fork: the transfer stream runs after the session's work so far
+  if (check_cuda(s, cudaEventRecord(s->x_fork, s->stream), "export fork") ||
+      check_cuda(s, cudaStreamWaitEvent(s->xs, s->x_fork, 0), "export fork"))
+    return s->err;
+  xport::k_export_count<<<(unsigned)((nsb + 7) / 8), 256, 0, s->xs>>>(f, blocks, sbs, (int)nsb, s->xcounts);
   if (after_launch(s, "export count")) return s->err;
-  xport::k_export_scan<<<1, xport::SCAN_THREADS, 0, s->stream>>>(
+  xport::k_export_scan<<<1, xport::SCAN_THREADS, 0, s->xs>>>(
       s->xcounts, (int)nsb, s->xblk_base, s->xcoef_base, s->xmeta, (const int8_t *)s->buf[MAV1CU_BUF_CDEF_CHOICE],
       dimg, layout, (long long)nsb * MAX_BLOCKS_PER_SB, (long long)nsb * COEFS_PER_SB);
   if (after_launch(s, "export scan")) return s->err;
-  xport::k_export_write<<<(unsigned)nsb, xport::WRITE_THREADS, 0, s->stream>>>(
-      DP(s), blocks, sbs, (const int32_t *)s->buf[MAV1CU_BUF_COEFS], s->xblk_base, s->xcoef_base, s->xmeta, dimg,
-      layout);
-  return after_launch(s, "export write");
+  xport::k_export_write<<<(unsigned)imin((int)nsb, xport::STORE_CTAS), xport::WRITE_THREADS, 0, s->xs>>>(
+      f, blocks, sbs, (int)nsb, (const int32_t *)s->buf[MAV1CU_BUF_COEFS], s->xblk_base, s->xcoef_base, s->xmeta,
+      dimg, layout);
+  if (after_launch(s, "export write")) return s->err;
+  if (withRec) {
+    const Geometry &g = s->g;
+    int rows = g.h + 2 * ((g.h + 1) >> 1);
+    xport::k_export_rec<<<imin(rows, xport::STORE_CTAS), 128, 0, s->xs>>>(
+        U8(s, MAV1CU_BUF_REC), make_int3(g.offset[0], g.offset[1], g.offset[2]),
+                                                 make_int2(g.stride[0], g.stride[1]), g.w, g.h, s->xmeta,
+                                                 dimg + layout.rec_off);
+    if (after_launch(s, "export reconstruction")) return s->err;
+  }
+  if (check_cuda(s, cudaEventRecord(s->x_done, s->xs), "export done")) return s->err;
+  s->x_pending = 1;
+  return MAV1CU_OK;
 }
+
 
 extern "C" int mav1cu_synchronize(mav1cu_session *s) {
   if (s->err) return s->err;
   if (check_cuda(s, cudaStreamSynchronize(s->stream), "synchronize")) return s->err;
+  if (check_cuda(s, cudaStreamSynchronize(s->xs), "synchronize transfers")) return s->err;
   int st[2] = {0, 0};
   if (check_cuda(s, cudaMemcpy(st, s->status, sizeof st, cudaMemcpyDeviceToHost), "status")) return s->err;
   if (st[0])
@@ -747,7 +801,12 @@ typedef std::shared_ptr<Event> EventRef;
 struct mav1cu_stream {
   drv::Norm n;
   mav1cu_session *eng[NUM_ENGINES];
-  uint8_t *staging[NUM_ENGINES];
+  // host sources: per engine, an upload stream and two staging buffers, so
+  // a frame's host->device copy overlaps the engine's previous frame
+  uint8_t *staging[NUM_ENGINES][2];
+  cudaStream_t upload[NUM_ENGINES];
+  cudaEvent_t up_done[NUM_ENGINES][2], load_done[NUM_ENGINES][2];
+  int up_next[NUM_ENGINES];
   uint8_t *slot[8];
   EventRef written[8];                // last write of each slot
   std::vector<EventRef> readers[8];   // reference copies of the slot's picture since then
@@ -780,7 +839,14 @@ extern "C" int mav1cu_stream_create(const mav1cu_config *cfg, mav1cu_stream **ou
     e = cudaMalloc(&st->slot[k], fb);
     if (e == cudaSuccess) e = cudaMemset(st->slot[k], 0, fb);
   }
-  for (int k = 0; k < NUM_ENGINES && e == cudaSuccess; k++) e = cudaMalloc(&st->staging[k], st->i420_bytes);
+  for (int k = 0; k < NUM_ENGINES && e == cudaSuccess; k++) {
+    for (int b = 0; b < 2 && e == cudaSuccess; b++) {
+      e = cudaMalloc(&st->staging[k][b], st->i420_bytes);
+      if (e == cudaSuccess) e = cudaEventCreateWithFlags(&st->up_done[k][b], cudaEventDisableTiming);
+      if (e == cudaSuccess) e = cudaEventCreateWithFlags(&st->load_done[k][b], cudaEventDisableTiming);
+    }
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&st->upload[k], cudaStreamNonBlocking);
+  }
   if (e == cudaSuccess) e = cudaDeviceSynchronize();
   if (e != cudaSuccess) {
     snprintf(err, errlen, "stream allocation failed: %s", cudaGetErrorString(e));
@@ -793,15 +859,22 @@ extern "C" int mav1cu_stream_create(const mav1cu_config *cfg, mav1cu_stream **ou
 
 extern "C" void mav1cu_stream_destroy(mav1cu_stream *st) {
   if (!st) return;
-  for (int e = 0; e < NUM_ENGINES; e++)
+  for (int e = 0; e < NUM_ENGINES; e++) {
+    if (st->upload[e]) cudaStreamSynchronize(st->upload[e]);
     if (st->eng[e]) cudaStreamSynchronize(st->eng[e]->stream);
+  }
   for (int k = 0; k < 8; k++) {
     st->written[k].reset();
     st->readers[k].clear();
     if (st->slot[k]) cudaFree(st->slot[k]);
   }
   for (int e = 0; e < NUM_ENGINES; e++) {
-    if (st->staging[e]) cudaFree(st->staging[e]);
+    for (int b = 0; b < 2; b++) {
+      if (st->staging[e][b]) cudaFree(st->staging[e][b]);
+      if (st->up_done[e][b]) cudaEventDestroy(st->up_done[e][b]);
+      if (st->load_done[e][b]) cudaEventDestroy(st->load_done[e][b]);
+    }
+    if (st->upload[e]) cudaStreamDestroy(st->upload[e]);
     mav1cu_session_destroy(st->eng[e]);
   }
   delete st;
@@ -819,20 +892,32 @@ extern "C" void *mav1cu_stream_slot(mav1cu_stream *st, int k) { return k >= 0 &&
 extern "C" int mav1cu_stream_wait(mav1cu_stream *st, void *stream) {
   Event ev;
   cudaEventRecord(ev.e, (cudaStream_t)stream);
-  for (int k = 0; k < NUM_ENGINES; k++) cudaStreamWaitEvent(st->eng[k]->stream, ev.e, 0);
+  for (int k = 0; k < NUM_ENGINES; k++) {
+    cudaStreamWaitEvent(st->eng[k]->stream, ev.e, 0);
+    cudaStreamWaitEvent(st->upload[k], ev.e, 0);
+  }
   return check_cuda(st->eng[0], cudaGetLastError(), "stream wait");
 }
+
+// The session's work so far, transfers included, precedes what `stream`
+// enqueues next.
+static void join_session(mav1cu_session *s, cudaStream_t stream) {
+  Event ev, evx;
+  cudaEventRecord(ev.e, s->stream);
+  cudaStreamWaitEvent(stream, ev.e, 0);
+  cudaEventRecord(evx.e, s->xs);
+  cudaStreamWaitEvent(stream, evx.e, 0);
+}
+
 extern "C" int mav1cu_stream_join(mav1cu_stream *st, void *stream) {
-  for (int k = 0; k < NUM_ENGINES; k++) {
-    Event ev;
-    cudaEventRecord(ev.e, st->eng[k]->stream);
-    cudaStreamWaitEvent((cudaStream_t)stream, ev.e, 0);
-  }
+  for (int k = 0; k < NUM_ENGINES; k++) join_session(st->eng[k], (cudaStream_t)stream);
   return check_cuda(st->eng[0], cudaGetLastError(), "stream join");
 }
 extern "C" int mav1cu_stream_synchronize(mav1cu_stream *st) {
-  for (int k = 0; k < NUM_ENGINES; k++)
+  for (int k = 0; k < NUM_ENGINES; k++) {
+    if (check_cuda(st->eng[k], cudaStreamSynchronize(st->upload[k]), "synchronize uploads")) return st->eng[k]->err;
     if (mav1cu_synchronize(st->eng[k])) return st->eng[k]->err;
+  }
   return MAV1CU_OK;
 }
 
@@ -852,15 +937,26 @@ extern "C" int mav1cu_stream_encode(mav1cu_stream *st, const mav1cu_frame_job *j
   st->last_engine = ei;
   size_t fb = s->g.frame_bytes;
   const uint8_t *src = (const uint8_t *)i420;
+  int b = -1;
   if (!on_device) {
-    if (check_cuda(s, cudaMemcpyAsync(st->staging[ei], i420, st->i420_bytes, cudaMemcpyHostToDevice, s->stream), "source upload"))
+    // upload stream: wait until the load that last read this staging buffer
+    // is done, copy, and let the engine wait for the copy
+    b = st->up_next[ei];
+    st->up_next[ei] ^= 1;
+    cudaStream_t us = st->upload[ei];
+    if (check_cuda(s, cudaStreamWaitEvent(us, st->load_done[ei][b], 0), "source upload") ||
+        check_cuda(s, cudaMemcpyAsync(st->staging[ei][b], i420, st->i420_bytes, cudaMemcpyHostToDevice, us),
+                   "source upload") ||
+        check_cuda(s, cudaEventRecord(st->up_done[ei][b], us), "source upload") ||
+        check_cuda(s, cudaStreamWaitEvent(s->stream, st->up_done[ei][b], 0), "source upload"))
       return s->err;
-    src = st->staging[ei];
+    src = st->staging[ei][b];
   }
   dim3 grid((s->g.stride[0] + 127) / 128, s->g.plane_h[0], 3);
   drv::k_load_source<<<grid, 128, 0, s->stream>>>(src, U8(s, MAV1CU_BUF_SRC), c.width, c.height, s->g.sb_cols,
                                                   s->g.sb_rows);
   if (after_launch(s, "load source")) return s->err;
+  if (b >= 0 && check_cuda(s, cudaEventRecord(st->load_done[ei][b], s->stream), "source upload")) return s->err;
   if (!job->is_key) {
     int refs[2] = {job->last_slot, job->arf_slot};
     int bufs[2] = {MAV1CU_BUF_REF, MAV1CU_BUF_GOLD};

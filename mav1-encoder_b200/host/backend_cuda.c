@@ -75,7 +75,7 @@ static size_t bsize(CudaBackend *cb, int buf) { return mav1cu_buf_size(cb->s, bu
 
 static void export_writer_inputs(CudaBackend *cb) {
   void *img = mav1cu_export_image(cb->s);
-  ok(cb, img ? mav1cu_export(cb->s, img, mav1cu_export_capacity(cb->s)) : MAV1CU_ERR_NOMEM);
+  ok(cb, img ? mav1cu_export(cb->s, img, mav1cu_export_capacity(cb->s), 0) : MAV1CU_ERR_NOMEM);
 }
 
 static void section(CudaBackend *cb, Buf *dst, const mav1cu_export_header *h, int64_t off, size_t n) {

@@ -56,8 +56,9 @@ assert PARAMS_DTYPE.itemsize == 392 and BLOCK_DTYPE.itemsize == 108
 EXPORT_HEADER_DTYPE = np.dtype([
     ("status", "<i4"), ("seq", "<i4"), ("num_sbs", "<i4"), ("num_blocks", "<i4"), ("num_coefs", "<i4"),
     ("zero_run", "<i4"), ("sbs_off", "<i8"), ("cdef_off", "<i8"), ("blocks_off", "<i8"), ("coefs_off", "<i8"),
-    ("bytes", "<i8")])
-assert SB_DTYPE.itemsize == 356 and LRUNIT_DTYPE.itemsize == 48 and EXPORT_HEADER_DTYPE.itemsize == 64
+    ("rec_off", "<i8"), ("rec_bytes", "<i8"), ("bytes", "<i8")])
+EXPORT_REC = 1
+assert SB_DTYPE.itemsize == 356 and LRUNIT_DTYPE.itemsize == 48 and EXPORT_HEADER_DTYPE.itemsize == 80
 
 EXPORTS = [
     "mav1cu_session_create", "mav1cu_session_destroy", "mav1cu_set_stream", "mav1cu_get_stream", "mav1cu_buf_size",
@@ -135,7 +136,7 @@ def load_library(path=LIB_PATH):
     lib.mav1cu_export_capacity.restype = sz
     lib.mav1cu_export_image.argtypes = [vp]
     lib.mav1cu_export_image.restype = vp
-    lib.mav1cu_export.argtypes = [vp, vp, sz]
+    lib.mav1cu_export.argtypes = [vp, vp, sz, i32]
     lib.mav1cu_export.restype = i32
     return lib
 
@@ -263,16 +264,17 @@ class Session:
     def export_capacity(self):
         return self.lib.mav1cu_export_capacity(self.h)
 
-    def export(self, image_ptr=None, cap=None):
-        """Enqueues the compact export of the writer inputs into image_ptr
-        (mapped page-locked host or device memory), or into the session's own
-        image; returns the image's address."""
+    def export(self, image_ptr=None, cap=None, rec=False):
+        """Enqueues the compact export of the writer inputs (and with rec the
+        shown reconstruction) into image_ptr (mapped page-locked host or
+        device memory), or into the session's own image; returns the image's
+        address."""
         if image_ptr is None:
             image_ptr = self.lib.mav1cu_export_image(self.h)
             if not image_ptr:
                 self._check(-2, "export image")
         cap = self.export_capacity() if cap is None else cap
-        self._check(self.lib.mav1cu_export(self.h, image_ptr, cap), "export")
+        self._check(self.lib.mav1cu_export(self.h, image_ptr, cap, EXPORT_REC if rec else 0), "export")
         return image_ptr
 
     def launches(self):
@@ -280,8 +282,9 @@ class Session:
 
 
 def export_sections(image):
-    """(header, superblocks, CDEF choices, blocks, levels) of an export image
-    held in a uint8 array."""
+    """(header, superblocks, CDEF choices, blocks, levels, reconstruction) of
+    an export image held in a uint8 array (reconstruction: None when the
+    export left it out)."""
     h = image[:EXPORT_HEADER_DTYPE.itemsize].view(EXPORT_HEADER_DTYPE)[0]
     if h["status"]:
         raise Mav1cuError(f"export image status {int(h['status'])}")
@@ -290,8 +293,9 @@ def export_sections(image):
     def sect(off, dtype, n):
         return image[int(off):int(off) + n * np.dtype(dtype).itemsize].view(dtype)
 
+    rec = sect(h["rec_off"], np.uint8, int(h["rec_bytes"])) if h["rec_bytes"] else None
     return (h, sect(h["sbs_off"], SB_DTYPE, nsb), sect(h["cdef_off"], np.int8, nsb),
-            sect(h["blocks_off"], BLOCK_DTYPE, nb), sect(h["coefs_off"], np.int32, nc))
+            sect(h["blocks_off"], BLOCK_DTYPE, nb), sect(h["coefs_off"], np.int32, nc), rec)
 
 
 def cli_config(width, height, q=100, keyint=0, lf=1, cdef=1, txs=1, txd=1, lr=1, lr_test=0, sw=1, fast=0, turbo=0,

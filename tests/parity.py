@@ -429,7 +429,7 @@ def pack_writer_inputs(blocks, sbs, coefs, cdef, p):
 def export_vs_packed(image, blocks, sbs, coefs, cdef, p):
     """Mismatch counts between an export image (uint8 array) and the packing
     of the dense buffers it was made from."""
-    h, isbs, icdef, iblocks, ilevels = mav1cu.export_sections(image)
+    h, isbs, icdef, iblocks, ilevels, irec = mav1cu.export_sections(image)
     want = pack_writer_inputs(blocks, sbs, coefs, cdef, p)
     out = dict(zero_run=int(h["zero_run"] != want["zero_run"]),
                num_blocks=int(h["num_blocks"] != len(want["blocks"])),
@@ -438,7 +438,7 @@ def export_vs_packed(image, blocks, sbs, coefs, cdef, p):
     out["cdef"] = int((icdef != want["cdef"]).sum())
     out["blocks"] = int((iblocks != want["blocks"]).sum()) if len(iblocks) == len(want["blocks"]) else -1
     out["levels"] = int((ilevels != want["levels"]).sum()) if len(ilevels) == len(want["levels"]) else -1
-    nbytes = (64 + len(isbs) * SB_DTYPE.itemsize + len(icdef) + len(iblocks) * BLOCK_DTYPE.itemsize +
-              4 * len(ilevels))
+    nbytes = (mav1cu.EXPORT_HEADER_DTYPE.itemsize + len(isbs) * SB_DTYPE.itemsize + len(icdef) +
+              len(iblocks) * BLOCK_DTYPE.itemsize + 4 * len(ilevels) + (0 if irec is None else len(irec)))
     out["bytes"] = int(h["bytes"] != nbytes)
     return out

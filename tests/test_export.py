@@ -6,8 +6,9 @@ its BLOCKS / SBS / COEFS buffers are replaced by the packed sections (the
 rest of each buffer filled with poison), and the bitstream must not change.
 
 GPU: the image the device writes into mapped host memory equals the packing
-of the dense buffers, frame by frame, through the device stream; a device
-memory image equals a host one; bad images are refused."""
+of the dense buffers, frame by frame, through the device stream, and its
+reconstruction section equals the visible samples of REC; a device memory
+image equals a host one; bad images are refused."""
 import ctypes
 
 import numpy as np
@@ -157,10 +158,10 @@ def test_stream_export_matches_packing(name, spec, flags):
         image = _pinned(cap)
         for k, job in enumerate(jobs):
             sess = st.encode(job, dframes[job["disp"]].data_ptr(), True)
-            sess.export(image.data_ptr(), cap)
+            sess.export(image.data_ptr(), cap, rec=not job["hidden"])
             st.synchronize()
             img = image.numpy().copy()
-            h = img[:64].view(mav1cu.EXPORT_HEADER_DTYPE)[0]
+            h = img[:mav1cu.EXPORT_HEADER_DTYPE.itemsize].view(mav1cu.EXPORT_HEADER_DTYPE)[0]
             assert h["status"] == 0 and h["num_sbs"] == sess.geom["num_sbs"]
             nsb = sess.geom["num_sbs"]
             blocks = sess.download("BLOCKS").view(BLOCK_DTYPE)
@@ -170,7 +171,13 @@ def test_stream_export_matches_packing(name, spec, flags):
             p = sess.download("PARAMS", count=PARAMS_DTYPE.itemsize).view(PARAMS_DTYPE)[0]
             bad = {k_: v for k_, v in parity.export_vs_packed(img, blocks, sbs, coefs, cdef, p).items() if v}
             assert not bad, (k, bad)
-            assert h["bytes"] < (nsb * (SB_DTYPE.itemsize + 64 * BLOCK_DTYPE.itemsize + 4 * 6144))
+            rec = mav1cu.export_sections(img)[5]
+            if job["hidden"]:
+                assert rec is None
+            else:
+                # mav1_get_recon's planes: the visible samples of REC
+                assert np.array_equal(rec, parity.visible(sess.download("REC"), sess.geom)), k
+            assert h["bytes"] - h["rec_bytes"] < (nsb * (SB_DTYPE.itemsize + 64 * BLOCK_DTYPE.itemsize + 4 * 6144))
     finally:
         st.close()
 
@@ -188,24 +195,25 @@ def test_device_image_equals_host_image_and_bad_images_are_refused():
         cap = sess.export_capacity()
         host = _pinned(cap)
         dev = torch.zeros(cap, dtype=torch.uint8, device="cuda")
-        sess.export(host.data_ptr(), cap)
-        sess.export(dev.data_ptr(), cap)
-        own = sess.export()
+        sess.export(host.data_ptr(), cap, rec=True)
+        sess.export(dev.data_ptr(), cap, rec=True)
+        own = sess.export(rec=True)
         st.synchronize()
         h = host.numpy()
-        n = int(h[:64].view(mav1cu.EXPORT_HEADER_DTYPE)[0]["bytes"])
+        n = int(h[:mav1cu.EXPORT_HEADER_DTYPE.itemsize].view(mav1cu.EXPORT_HEADER_DTYPE)[0]["bytes"])
         d = dev.cpu().numpy()
         o = np.ctypeslib.as_array(ctypes.cast(own, ctypes.POINTER(ctypes.c_uint8)), shape=(cap,))
-        hdr = [x[:64].view(mav1cu.EXPORT_HEADER_DTYPE)[0] for x in (h, d, o)]
+        hdr = [x[:mav1cu.EXPORT_HEADER_DTYPE.itemsize].view(mav1cu.EXPORT_HEADER_DTYPE)[0] for x in (h, d, o)]
         assert [int(x["seq"]) for x in hdr] == [1, 2, 3]
         for a, b in zip(mav1cu.export_sections(h)[1:], mav1cu.export_sections(d)[1:]):
             assert np.array_equal(a, b)
         for a, b in zip(mav1cu.export_sections(h)[1:], mav1cu.export_sections(o)[1:]):
             assert np.array_equal(a, b)
+        assert mav1cu.export_sections(h)[5] is not None
         assert n > 0
         # refused before any device work: too small, unaligned, pageable host memory
         lib = sess.lib
-        assert lib.mav1cu_export(sess.h, host.data_ptr(), cap - 1) == -1
+        assert lib.mav1cu_export(sess.h, host.data_ptr(), cap - 1, 0) == -1
     finally:
         st.close()
     st = mav1cu.Stream(cfg)
@@ -213,7 +221,7 @@ def test_device_image_equals_host_image_and_bad_images_are_refused():
         sess = st.encode(jobs[0], torch.from_numpy(frames[jobs[0]["disp"]]).cuda().data_ptr(), True)
         cap = sess.export_capacity()
         host = _pinned(cap + 64)
-        assert sess.lib.mav1cu_export(sess.h, host.data_ptr() + 4, cap) == -1
+        assert sess.lib.mav1cu_export(sess.h, host.data_ptr() + 4, cap, 0) == -1
     finally:
         st.close()
     st = mav1cu.Stream(cfg)
@@ -222,7 +230,7 @@ def test_device_image_equals_host_image_and_bad_images_are_refused():
         cap = sess.export_capacity()
         pageable = np.zeros(cap + 64, np.uint8)
         addr = (pageable.ctypes.data + 15) & ~15
-        assert sess.lib.mav1cu_export(sess.h, addr, cap) == -1
+        assert sess.lib.mav1cu_export(sess.h, addr, cap, 0) == -1
         assert b"neither mapped" in sess.lib.mav1cu_error_string(sess.h)
     finally:
         st.close()
