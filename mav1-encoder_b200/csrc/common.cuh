@@ -13,8 +13,10 @@
 
 #if defined(__CUDACC__)
 #define HD __host__ __device__ __forceinline__
+#define HDM __host__ __device__ __forceinline__
 #else
 #define HD static inline
+#define HDM inline
 #endif
 
 typedef mav1cu_frame_params FrameParams;

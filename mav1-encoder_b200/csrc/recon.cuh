@@ -228,7 +228,7 @@ __device__ void inv_row_split(Smem &sm, const int32_t *q, int i, int half, int t
     for (int k = 0; k < HW; k++) t[k] = (int32_t)round2l((int64_t)t[k] * 2896, 12);
   }
   if (half == 0) tx::idct<LW - 1, false>(t, 16);
-  else tx::idct_odd<LW>(t - HW, 16);
+  else tx::idct_odd<LW>(t, 16);
 #pragma unroll
   for (int k = 0; k < HW; k++) row[k + half * HW] = t[k];
   __syncwarp(pair);
@@ -251,7 +251,7 @@ __device__ void inv_col_split(Smem &sm, int j, int half, int w, int fud, int flr
   for (int k = 0; k < HH; k++) t[k] = sm.resid[tx::brev(LH, k + half * HH) * 64 + j];
   __syncwarp(pair);  // both halves read before the column is overwritten
   if (half == 0) tx::idct<LH - 1, false>(t, 16);
-  else tx::idct_odd<LH>(t - HH, 16);
+  else tx::idct_odd<LH>(t, 16);
 #pragma unroll
   for (int k = 0; k < HH; k++) sm.resid[(k + half * HH) * 64 + j] = t[k];
   __syncwarp(pair);

@@ -28,8 +28,10 @@ HD int cos128(int angle) {
 }
 HD int sin128(int angle) { return cos128(angle - 64); }
 
-// Butterfly rotation B( a, b, angle, flip ) (spec 7.13.2.1).
-HD void B(int32_t *t, int a, int b, int angle, int flip) {
+// Butterfly rotation B( a, b, angle, flip ) (spec 7.13.2.1). T_ is an
+// int32_t pointer or an Offset view.
+template <class T_>
+HD void B(T_ t, int a, int b, int angle, int flip) {
   int64_t c = cos128(angle), s = sin128(angle);
   int64_t x = (int64_t)t[a] * c - (int64_t)t[b] * s;
   int64_t y = (int64_t)t[a] * s + (int64_t)t[b] * c;
@@ -39,13 +41,21 @@ HD void B(int32_t *t, int a, int b, int angle, int flip) {
 }
 
 // Hadamard rotation H( a, b, flip, r ) with the r-bit clamp (spec 7.13.2.1).
-HD void H(int32_t *t, int a, int b, int flip, int r) {
+template <class T_>
+HD void H(T_ t, int a, int b, int flip, int r) {
   int ia = flip ? b : a, ib = flip ? a : b;
   int32_t x = t[ia], y = t[ib];
   int lo = -(1 << (r - 1)), hi = (1 << (r - 1)) - 1;
   t[ia] = clip3(lo, hi, x + y);
   t[ib] = clip3(lo, hi, x - y);
 }
+
+// Elements O, O+1, ... of a length-2O vector held from p: t[i] is p[i - O].
+template <int O>
+struct Offset {
+  int32_t *p;
+  HDM int32_t &operator[](int i) const { return p[i - O]; }
+};
 
 // Inverse DCT of length 1 << N (spec 7.13.2.3).
 template <int N, bool PERM = true>
@@ -197,12 +207,14 @@ HD void idct(int32_t *t, int r) {
 // threads. After the input permutation, the operations of idct<N> on
 // elements 0 .. n0/2 - 1 are exactly idct<N - 1> without its permutation,
 // and those on n0/2 .. n0 - 1 are the groups that only N adds (idct_odd,
-// the same operations in the same order; t points at element 0, so the odd
-// half is t[n0/2 ..]); the halves touch disjoint elements until the last
-// stage, H(i, n0 - 1 - i) for i < n0/2 (idct_join_pair). Running the
-// halves concurrently and then the join gives idct<N>'s result exactly.
+// the same operations in the same order, on element indices n0/2 .. n0 - 1;
+// `odd` holds those elements, odd[0] being element n0/2); the halves touch
+// disjoint elements until the last stage, H(i, n0 - 1 - i) for i < n0/2
+// (idct_join_pair). Running the halves concurrently and then the join gives
+// idct<N>'s result exactly.
 template <int N>
-HD void idct_odd(int32_t *t, int r) {
+HD void idct_odd(int32_t *odd, int r) {
+  Offset<(1 << N) / 2> t{odd};
   if (N == 6) {
 #pragma unroll
     for (int i = 0; i < 16; i++) B(t, 32 + i, 63 - i, 63 - 4 * brev(4, i), 0);

@@ -26,7 +26,7 @@ static int mismatches(std::mt19937 &g, int trials) {
       b[k] = in[tx::brev(N, k + h)];
     }
     tx::idct<N - 1, false>(a, 16);
-    tx::idct_odd<N>(b - h, 16);
+    tx::idct_odd<N>(b, 16);
     for (int k = 0; k < h; k++) {
       out[k] = a[k];
       out[k + h] = b[k];
