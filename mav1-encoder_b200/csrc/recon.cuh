@@ -1378,6 +1378,11 @@ __global__ void __launch_bounds__(128) k_block_deps(Ctx c, const int *list, cons
 }
 
 // Claim state of the recon launch: the list, its length and the counter.
+#ifndef MAV1CU_BLOCKS_PER_WORKER
+#define MAV1CU_BLOCKS_PER_WORKER 8
+#endif
+constexpr int BLOCKS_PER_WORKER = MAV1CU_BLOCKS_PER_WORKER, MIN_WORKERS = 8;
+
 struct Claim {
   const int *list;
   const int *total;
@@ -1389,11 +1394,16 @@ struct Claim {
 // its intra edges read) and publishes its completion flag.
 __global__ void __launch_bounds__(INTRA_THREADS, 1) k_recon_blocks(Ctx cg, Claim q) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  // workers in proportion to the frame's intra blocks: the surplus CTAs
+  // leave at once, so their SMs' registers and shared memory go to the other
+  // engines' kernels (an ALTREF frame has a few hundred intra blocks, a key
+  // frame tens of thousands)
+  int total = *q.total;
+  if (blockIdx.x >= imax(MIN_WORKERS, total / BLOCKS_PER_WORKER)) return;
   Smem &sm = *(Smem *)smem_raw;
   const Ctx c = load_shared(cg, sm);
   const FrameParams *fp = c.fp;
   volatile int *vstatus = c.status;
-  int total = *q.total;
   for (;;) {
     if (threadIdx.x == 0) {
       int slot = vstatus[1] ? total : atomicAdd(q.next, 1), me = -1;
