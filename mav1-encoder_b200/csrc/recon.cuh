@@ -82,9 +82,6 @@ struct Smem {
   int32_t tmp[64 * 32];    // forward row pass output
   int32_t q[32 * 32];      // levels of the current candidate
   int32_t qbest[32 * 32];  // levels kept by the tx type search
-  int edge[3][EDGE_LEN];   // AboveRow, LeftCol, filter copy
-  uint8_t save[64 * 64];
-  int16_t pred0[64 * 64];  // first compound prediction (intermediate precision)
   int sse33[33];
   long long red[INTER_THREADS / 32];
   BlockInfo blk;
@@ -104,14 +101,28 @@ struct Smem {
   int cornerAR[3], cornerBL[3];  // BlockDecoded of those units
   int32_t fmat[3][FMAT_SMALL];  // forward matrices of lengths 4, 8, 16 per kind
   int32_t fmatT[3][FMAT_SMALL]; // the same transposed
-  // intra block tiles: rows and columns -1 .. 2n - 1 around the block (its
-  // own samples, the above row over the above-right units, the left column
-  // over the below-left units), and its source
-  uint8_t tileY[TILE_Y * 129];
-  uint8_t tileC[2][TILE_C * 65];
-  uint8_t srcY[64 * 64];
-  uint8_t srcC[2][32 * 32];
+  // What only one of the two kernels uses. k_recon_inter launches with the
+  // shared memory up to the end of pred0 (SMEM_INTER), k_recon_blocks with
+  // the whole struct, so neither holds the other's part on its SMs.
+  union {
+    struct {  // inter blocks
+      int16_t pred0[64 * 64];  // first compound prediction (intermediate precision)
+    };
+    struct {  // intra blocks
+      int edge[3][EDGE_LEN];   // AboveRow, LeftCol, filter copy
+      uint8_t save[64 * 64];   // the block's luma before the tx_depth candidates
+      // tiles: rows and columns -1 .. 2n - 1 around the block (its own
+      // samples, the above row over the above-right units, the left column
+      // over the below-left units), and its source
+      uint8_t tileY[TILE_Y * 129];
+      uint8_t tileC[2][TILE_C * 65];
+      uint8_t srcY[64 * 64];
+      uint8_t srcC[2][32 * 32];
+    };
+  };
 };
+constexpr size_t SMEM_INTER = offsetof(Smem, pred0) + sizeof(int16_t) * 64 * 64;
+constexpr size_t SMEM_INTRA = sizeof(Smem);
 
 // Sums / maxima over the CTA. A one-warp CTA reduces by shuffles alone; the
 // __syncwarp()s order the shared-memory writes before and after like the

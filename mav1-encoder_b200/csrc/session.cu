@@ -342,13 +342,13 @@ extern "C" int mav1cu_session_create(int width, int height, int max_cdef_presets
     mav1cu_session_destroy(s);
     return code;
   }
-  cudaFuncSetAttribute(rec::k_recon_blocks, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(rec::Smem));
-  cudaFuncSetAttribute(rec::k_recon_inter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(rec::Smem));
+  cudaFuncSetAttribute(rec::k_recon_blocks, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rec::SMEM_INTRA);
+  cudaFuncSetAttribute(rec::k_recon_inter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rec::SMEM_INTER);
   {
     int dev = 0, sms = 0, per = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, rec::k_recon_blocks, rec::INTRA_THREADS, sizeof(rec::Smem));
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, rec::k_recon_blocks, rec::INTRA_THREADS, rec::SMEM_INTRA);
     // one worker per SM: the ready queue keeps them on ready blocks, and the
     // rest of each SM stays free for the other engines' kernels
     s->resident_recon = imax(1, sms * imin(1, imax(1, per)));
@@ -562,7 +562,7 @@ extern "C" int mav1cu_recon(mav1cu_session *s) {
                  "recon flags"))
     return s->err;
   if (!s->fp.frame_is_intra) {
-    rec::k_recon_inter<<<nsb, rec::INTER_THREADS, sizeof(rec::Smem), s->stream>>>(c);
+    rec::k_recon_inter<<<nsb, rec::INTER_THREADS, rec::SMEM_INTER, s->stream>>>(c);
     if (after_launch(s, "recon inter blocks")) return s->err;
   }
   // leaf frames code inter blocks only (the analysis never keeps intra there)
@@ -590,7 +590,7 @@ extern "C" int mav1cu_recon(mav1cu_session *s) {
   q.list = s->blk_list;
   q.total = s->status + 3;
   q.next = s->status + 2;
-  rec::k_recon_blocks<<<s->resident_recon, rec::INTRA_THREADS, sizeof(rec::Smem), s->stream>>>(c, q);
+  rec::k_recon_blocks<<<s->resident_recon, rec::INTRA_THREADS, rec::SMEM_INTRA, s->stream>>>(c, q);
   return after_launch(s, "recon intra blocks");
 }
 
