@@ -38,7 +38,10 @@ namespace rec {
 // Threads of the CTA coding a block: INTER_THREADS for the inter blocks of a
 // superblock, INTRA_THREADS for an intra block worker.
 #define RT ((int)blockDim.x)
-constexpr int INTER_THREADS = 256, INTRA_THREADS = 128;
+#ifndef MAV1CU_INTER_THREADS
+#define MAV1CU_INTER_THREADS 128
+#endif
+constexpr int INTER_THREADS = MAV1CU_INTER_THREADS, INTRA_THREADS = 128;
 #define FWD_SLOT_SIZE 4096
 HD int fwd_slot(int kind, int log2n) { return (kind * 5 + log2n - 2) * FWD_SLOT_SIZE; }
 
@@ -1307,7 +1310,7 @@ __device__ Ctx load_shared(const Ctx &c, Smem &sm) {
 // The inter blocks of the frame, one CTA per superblock (all at once: they
 // read reference pictures only), each published complete for the intra
 // workers that read its samples.
-__global__ void __launch_bounds__(INTER_THREADS, 2) k_recon_inter(Ctx cg) {
+__global__ void __launch_bounds__(INTER_THREADS, 512 / INTER_THREADS) k_recon_inter(Ctx cg) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Smem &sm = *(Smem *)smem_raw;
   const Ctx c = load_shared(cg, sm);
