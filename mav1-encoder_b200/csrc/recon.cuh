@@ -70,10 +70,16 @@ struct Ctx {
   int *done;            // per block index: 1 once its luma samples are written; then the same for chroma
   // the intra blocks' ready queue: unfinished luma dependencies per block,
   // successor lists (blocks whose luma edges read this block's luma), and
-  // the queue of blocks whose luma dependencies are all complete
+  // the queue of blocks whose luma dependencies are all complete (slot
+  // value: block index + 1; 0 while the slot is unfilled)
   int *dep_count, *succ_count, *succ;
-  int *queue, *qvalid, *qtail;
+  int *queue, *qtail;
+  // per intra block, BlockDecoded of its corner units: bit 0 / 1 luma
+  // above-right / below-left, bit 2 / 3 the same for chroma
+  int *corners;
 };
+
+#define MAX_SUCC 96  // successors per block: at most 25 along each edge, with margin
 
 #define TILE_OFF 4     // tile column of the block's first sample (word aligned; the left column at 3)
 #define TILE_Y 132     // luma tile stride: TILE_OFF + 2 * 64; rows -1 .. 127
@@ -100,7 +106,6 @@ struct Smem {
   const uint8_t *srcp[3];
   int sstride[3];
   FrameParams fpc;           // the CTA's copy of the frame parameters
-  int cornerBlk[6];          // block index at the above-right / below-left corner unit per plane (-1: none)
   int cornerAR[3], cornerBL[3];  // BlockDecoded of those units
   int32_t fmat[3][FMAT_SMALL];  // forward matrices of lengths 4, 8, 16 per kind
   int32_t fmatT[3][FMAT_SMALL]; // the same transposed
@@ -112,6 +117,9 @@ struct Smem {
       int16_t pred0[64 * 64];  // first compound prediction (intermediate precision)
     };
     struct {  // intra blocks
+      int cbits;               // the block's corner bits (Ctx::corners)
+      int succN;               // its successor count and list, copied while staging
+      int succ[MAX_SUCC];
       int edge[3][EDGE_LEN];   // AboveRow, LeftCol, filter copy
       uint8_t save[64 * 64];   // the block's luma before the tx_depth candidates
       // tiles: rows and columns -1 .. 2n - 1 around the block (its own
@@ -661,7 +669,7 @@ __device__ __forceinline__ int corner_decoded(const FrameParams *fp, const int *
   return blk >= 0 && blk < me;
 }
 
-// The edge samples plane p of block b can read (see stage_edges): row ay
+// The edge samples plane p of block b can read (see stage_chroma_edges): row ay
 // from ax0 to ax1 and column x0 - 1 from ly0 to ly1 (empty runs: end <
 // start), and the 4x4 luma units under them as two runs (ur, uc, urow, un).
 struct EdgeRuns {
@@ -802,15 +810,34 @@ __device__ void copy_segs(const CopySeg *sg) {
   }
 }
 
-// Stages an intra block in shared memory, first part: the block's own
-// samples of every plane (the reconstruction so far, overwritten as it is
-// coded), its source and its corner units' block indices, in one batch of
-// copies; the views then point at the tiles.
+// The copies of plane p's edge samples (edge runs e, see stage_chroma_edges)
+// into its tile: the row above from the word holding its first sample, and
+// the column left as the word ending at it, one per row.
+__device__ __forceinline__ void edge_segs(const Ctx &c, Smem &sm, int p, const EdgeRuns &e, CopySeg *sg) {
+  const FrameParams *fp = c.fp;
+  const BlockInfo &b = sm.blk;
+  int sub = p > 0, S = sub ? TILE_C : TILE_Y;
+  uint8_t *t = sub ? sm.tileC[p - 1] : sm.tileY;
+  int x0 = (b.mi_col >> sub) * 4, y0 = (b.mi_row >> sub) * 4, fs = fp->stride[p];
+  const uint8_t *g = c.rec + fp->offset[p];
+  int xs = e.ax0 & ~3;
+  sg[0] = CopySeg{t + xs - x0 + TILE_OFF, g + e.ay * fs + xs, 0, 0, e.ax1 >= e.ax0 ? ((e.ax1 - xs) >> 2) + 1 : 0, 20};
+  sg[1] = CopySeg{t + (e.ly0 - y0 + 1) * S + TILE_OFF - 4, g + e.ly0 * fs + x0 - 4, S, fs,
+                  e.ly1 >= e.ly0 ? e.ly1 - e.ly0 + 1 : 0, 0};
+}
+
+// Stages an intra block in shared memory, in one batch of copies: the
+// block's own samples of every plane (the reconstruction so far, overwritten
+// as it is coded), its source, its luma edge samples and its successor list.
+// The luma edges are complete: the ready queue hands out a block only once
+// every block under them has published its luma (k_block_deps). The corner
+// units' BlockDecoded come from the prepass (sm.cbits); the views then point
+// at the tiles.
 __device__ void stage_begin(const Ctx &c, Smem &sm) {
   const FrameParams *fp = c.fp;
   const BlockInfo &b = sm.blk;
-  int bs = b.bsize, tid = threadIdx.x;
-  CopySeg sg[12];
+  int bs = b.bsize, tid = threadIdx.x, cb = sm.cbits;
+  CopySeg sg[10];
   int ns = 0;
   for (int p = 0; p < 3; p++) {
     int sub = p > 0, S = sub ? TILE_C : TILE_Y;
@@ -819,17 +846,6 @@ __device__ void stage_begin(const Ctx &c, Smem &sm) {
     int x0 = (b.mi_col >> sub) * 4, y0 = (b.mi_row >> sub) * 4, fs = fp->stride[p];
     sg[ns++] = CopySeg{t + S + TILE_OFF, c.rec + fp->offset[p] + y0 * fs + x0, S, fs, (w >> 2) * h, lw - 2};
     sg[ns++] = CopySeg{sb, c.src + fp->offset[p] + y0 * fs + x0, w, fs, (w >> 2) * h, lw - 2};
-    // the corner units: above-right (top - 1, right), below-left (bottom, left - 1)
-    int top = (b.mi_row & 15) >> sub, left = (b.mi_col & 15) >> sub, n = 16 >> sub;
-    int bottom = top + (h >> 2), right = left + (w >> 2);
-    for (int k = 0; k < 2; k++) {
-      int y = k ? bottom : top - 1, x = k ? left - 1 : right;
-      int r = sm.r0 + (y << sub), col = sm.c0 + (x << sub);
-      int inside = y >= 0 && x >= 0 && y < n && x < n && r < fp->mi_rows && col < fp->mi_cols;
-      if (tid == 0) sm.cornerBlk[2 * p + k] = -1;
-      sg[ns++] = CopySeg{(uint8_t *)&sm.cornerBlk[2 * p + k], (const uint8_t *)(c.blk_at + r * fp->mi_cols + col), 0, 0,
-                         inside, 0};
-    }
     if (tid == 0) {
       sm.recp[p] = t + S + TILE_OFF - ((ptrdiff_t)y0 * S + x0);
       sm.rstride[p] = S;
@@ -837,79 +853,47 @@ __device__ void stage_begin(const Ctx &c, Smem &sm) {
       sm.sstride[p] = w;
     }
   }
-  __syncthreads();
-  copy_segs<12>(sg);
-  __syncthreads();
-  if (tid < 6) {
-    int p = tid >> 1, k = tid & 1, sub = p > 0, n = 16 >> sub;
-    int h = block_h(bs) >> sub, w = block_w(bs) >> sub;
-    int top = (b.mi_row & 15) >> sub, left = (b.mi_col & 15) >> sub;
-    int y = k ? top + (h >> 2) : top - 1, x = k ? left - 1 : left + (w >> 2);
-    int v;
-    if (y < 0 || x < 0 || y >= n || x >= n) {
-      v = decoded_outside(fp, sm.r0, sm.c0, sub, y, x);
-    } else {
-      int blk = sm.cornerBlk[tid];
-      v = blk >= 0 && blk < sm.me;  // -1: beyond the frame
-    }
-    if (k) sm.cornerBL[p] = v;
-    else sm.cornerAR[p] = v;
+  if (tid < 3) {
+    int sh = tid ? 2 : 0;
+    sm.cornerAR[tid] = (cb >> sh) & 1;
+    sm.cornerBL[tid] = (cb >> (sh + 1)) & 1;
   }
+  edge_segs(c, sm, 0, edge_runs(fp, b, 0, cb & 1, (cb >> 1) & 1), sg + ns);
+  ns += 2;
+  sg[ns++] = CopySeg{(uint8_t *)sm.succ, (const uint8_t *)(c.succ + (size_t)sm.me * MAX_SUCC), 0, 0, MAX_SUCC, 20};
+  sg[ns++] = CopySeg{(uint8_t *)&sm.succN, (const uint8_t *)(c.succ_count + sm.me), 0, 0, 1, 0};
+  copy_segs<10>(sg);
   __syncthreads();
 }
 
-// Second part, per plane group (0: luma, 1: both chroma planes): once the
-// blocks that wrote them have completed those planes, the edge samples the
-// group's transform blocks can read. Those are the row above and the
-// column left of the block, extended past its corner by the largest
-// candidate transform's shorter side where the above-right / below-left
-// unit is decoded: the union of the samples intra_edges reads (above / left
-// limits, spec 7.11.2) over every transform block of every candidate size.
-// Copies move whole aligned words (a word of the row above or of the
-// column left may carry samples no transform block reads).
-__device__ void stage_edges(const Ctx &c, Smem &sm, int group) {
+// The chroma planes' edge samples, once the blocks that wrote them have
+// completed their chroma. Those are the row above and the column left of the
+// block, extended past its corner by the largest candidate transform's
+// shorter side where the above-right / below-left unit is decoded: the union
+// of the samples intra_edges reads (above / left limits, spec 7.11.2) over
+// every transform block of every candidate size. Copies move whole aligned
+// words (a word of the row above or of the column left may carry samples no
+// transform block reads). The luma edges are staged with the block.
+__device__ void stage_chroma_edges(const Ctx &c, Smem &sm) {
   const FrameParams *fp = c.fp;
   const BlockInfo &b = sm.blk;
-  int p0 = group ? 1 : 0, np = group ? 2 : 1;
-  int ay[2], ax0[2], ax1[2], ly0[2], ly1[2];
+  EdgeRuns e[2];
   int ur[6] = {0}, uc[6] = {0}, urow[6] = {0}, un[6] = {0};  // the 4x4 luma units under the edge samples
-  for (int q = 0; q < np; q++) {
-    int p = p0 + q;
-    EdgeRuns e = edge_runs(fp, b, p, sm.cornerAR[p], sm.cornerBL[p]);
-    ay[q] = e.ay;
-    ax0[q] = e.ax0;
-    ax1[q] = e.ax1;
-    ly0[q] = e.ly0;
-    ly1[q] = e.ly1;
+  for (int q = 0; q < 2; q++) {
+    e[q] = edge_runs(fp, b, 1 + q, sm.cornerAR[1 + q], sm.cornerBL[1 + q]);
     for (int k = 0; k < 2; k++) {
-      ur[2 * q + k] = e.ur[k];
-      uc[2 * q + k] = e.uc[k];
-      urow[2 * q + k] = e.urow[k];
-      un[2 * q + k] = e.un[k];
+      ur[2 * q + k] = e[q].ur[k];
+      uc[2 * q + k] = e[q].uc[k];
+      urow[2 * q + k] = e[q].urow[k];
+      un[2 * q + k] = e[q].un[k];
     }
   }
-  // luma: the ready queue hands out a block only once every block its luma
-  // edges read has published its luma (k_block_deps); chroma: wait here
-  if (group) wait_units(c, sm, group, ur, uc, urow, un);
+  wait_units(c, sm, 1, ur, uc, urow, un);
   __threadfence();
   __syncthreads();
   CopySeg sg[4];
-  for (int q = 0; q < 2; q++) {
-    if (q >= np) {
-      sg[2 * q] = sg[2 * q + 1] = CopySeg{nullptr, nullptr, 0, 0, 0, 0};
-      continue;
-    }
-    int p = p0 + q, sub = p > 0, S = sub ? TILE_C : TILE_Y;
-    uint8_t *t = sub ? sm.tileC[p - 1] : sm.tileY;
-    int x0 = (b.mi_col >> sub) * 4, y0 = (b.mi_row >> sub) * 4, fs = fp->stride[p];
-    const uint8_t *g = c.rec + fp->offset[p];
-    int xs = ax0[q] & ~3;  // the row above, from the word holding its first sample
-    sg[2 * q] = CopySeg{t + xs - x0 + TILE_OFF, g + ay[q] * fs + xs, 0, 0,
-                        ax1[q] >= ax0[q] ? ((ax1[q] - xs) >> 2) + 1 : 0, 20};
-    // the column left: the word ending at it, one per row
-    sg[2 * q + 1] = CopySeg{t + (ly0[q] - y0 + 1) * S + TILE_OFF - 4, g + ly0[q] * fs + x0 - 4, S, fs,
-                            ly1[q] >= ly0[q] ? ly1[q] - ly0[q] + 1 : 0, 0};
-  }
+  edge_segs(c, sm, 1, e[0], sg);
+  edge_segs(c, sm, 2, e[1], sg + 2);
   copy_segs<4>(sg);
   __syncthreads();
 }
@@ -1088,22 +1072,20 @@ __device__ void predict_block(Smem &sm, const pred::Inter &ip, int lw, int h, in
   __syncthreads();
 }
 
-#define MAX_SUCC 96  // successors per block: at most 25 along each edge, with margin
 
 // Appends a block whose luma dependencies are complete to the ready queue.
 __device__ __forceinline__ void push_ready(const Ctx &c, int blk) {
   int t = atomicAdd(c.qtail, 1);
-  c.queue[t] = blk;
-  __threadfence();
-  atomicExch(c.qvalid + t, 1);
+  __threadfence();  // the luma this release follows is visible before the slot fills
+  atomicExch(c.queue + t, blk + 1);
 }
 
 // After this block's luma is published: one dependency fewer for each
 // successor; the last one releases it to the ready queue.
 __device__ void release_successors(const Ctx &c, const Smem &sm) {
-  int n = imin(c.succ_count[sm.me], MAX_SUCC);
+  int n = imin(sm.succN, MAX_SUCC);  // the list staged with the block
   for (int k = threadIdx.x; k < n; k += RT) {
-    int s = c.succ[sm.me * MAX_SUCC + k];
+    int s = sm.succ[k];
     if (atomicSub(c.dep_count + s, 1) == 1) push_ready(c, s);
   }
 }
@@ -1131,10 +1113,7 @@ __device__ void recon_block(const Ctx &c, Smem &sm, BlockInfo *gb) {
     sm.sstride[p] = fp->stride[p];
   }
   __syncthreads();
-  if (!INTER) {
-    stage_begin(c, sm);
-    stage_edges(c, sm, 0);
-  }
+  if (!INTER) stage_begin(c, sm);
   int tid = threadIdx.x;
   if (INTER && fp->switchable_interp && !comp) {
     int w = block_w(bs), h = block_h(bs);
@@ -1174,7 +1153,7 @@ __device__ void recon_block(const Ctx &c, Smem &sm, BlockInfo *gb) {
       // while this one codes its chroma
       unstage_intra(c, sm, 0, 1);
       release_successors(c, sm);
-      stage_edges(c, sm, 1);
+      stage_chroma_edges(c, sm);
     }
     int sub = plane > 0, stride = fp->stride[plane];
     int baseX = (MiCol >> sub) * 4, baseY = (MiRow >> sub) * 4;
@@ -1349,9 +1328,13 @@ __global__ void __launch_bounds__(128) k_block_deps(Ctx c, const int *list, cons
     BlockInfo b = c.blocks[me];
     int sb = me / MAX_BLOCKS_PER_SB, r0 = (sb / fp->sb_cols) * 16, c0 = (sb % fp->sb_cols) * 16;
     EdgeRuns e[2];  // luma; chroma (both chroma planes share their geometry)
-    for (int p = 0; p < 2; p++)
-      e[p] = edge_runs(fp, b, p, corner_decoded(fp, c.blk_at, b, me, r0, c0, p, 0),
-                       corner_decoded(fp, c.blk_at, b, me, r0, c0, p, 1));
+    int cb = 0;
+    for (int p = 0; p < 2; p++) {
+      int ar = corner_decoded(fp, c.blk_at, b, me, r0, c0, p, 0), bl = corner_decoded(fp, c.blk_at, b, me, r0, c0, p, 1);
+      e[p] = edge_runs(fp, b, p, ar, bl);
+      cb |= (ar | bl << 1) << (2 * p);
+    }
+    if (lane == 0) c.corners[me] = cb;
     int run[4] = {e[0].un[0], e[0].un[1], e[1].un[0], e[1].un[1]};
     int n = imin(160, run[0] + run[1] + run[2] + run[3]);
     int nblk = fp->sb_cols * fp->sb_rows * MAX_BLOCKS_PER_SB;
@@ -1424,9 +1407,9 @@ __global__ void __launch_bounds__(INTRA_THREADS, 1) k_recon_blocks(Ctx cg, Claim
       if (slot < total) {
         // the slot fills once its block is released (every block is, once
         // the blocks before it in any dependency chain complete)
-        volatile int *vvalid = c.qvalid + slot;
+        volatile int *vslot = c.queue + slot;
         int spins = 0;
-        while (!*vvalid && !vstatus[1]) {
+        while (!*vslot && !vstatus[1]) {
           if (++spins > SPIN_LIMIT) {
             atomicExch(c.status, 1);
             atomicExch(c.status + 1, 1);
@@ -1435,7 +1418,7 @@ __global__ void __launch_bounds__(INTRA_THREADS, 1) k_recon_blocks(Ctx cg, Claim
           __nanosleep(64);
         }
         __threadfence();
-        if (*vvalid) me = ((volatile int *)c.queue)[slot];
+        me = *vslot - 1;
       }
       sm.flag = me;
       if (me >= 0) {
@@ -1444,6 +1427,7 @@ __global__ void __launch_bounds__(INTRA_THREADS, 1) k_recon_blocks(Ctx cg, Claim
         sm.r0 = (sb / fp->sb_cols) * 16;
         sm.c0 = (sb % fp->sb_cols) * 16;
         sm.blk = c.blocks[me];
+        sm.cbits = c.corners[me];
       }
     }
     __syncthreads();

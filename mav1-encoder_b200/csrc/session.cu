@@ -77,7 +77,7 @@ struct mav1cu_session {
   int *blk_at;             // block index per 4x4 luma unit
   int *blk_list;           // recon claim list
   int *blk_done;           // per-block completion flags of the recon launch: luma, then chroma
-  int *dep_count, *succ_count, *succ, *queue, *qvalid;  // intra ready queue (rec::Ctx)
+  int *dep_count, *succ_count, *succ, *queue, *corners;  // intra ready queue and corner bits (rec::Ctx)
   int resident_recon;      // intra recon workers (CTAs, one per SM)
   int4 *xcounts;           // compact export: per-superblock counts, block and level bases, zero run / fit flag
   int *xblk_base, *xcoef_base, *xmeta;
@@ -253,7 +253,7 @@ static void free_all(mav1cu_session *s) {
   for (int i = 0; i < MAV1CU_BUF_COUNT; i++)
     if (s->buf[i]) cudaFree(s->buf[i]);
   void *extra[] = {s->qp[0], s->qp[1], s->dsrc, s->dref[0], s->dref[1], s->ys, s->uvs, s->waves, s->status, s->blk_at, s->blk_list,
-                   s->blk_done, s->mats_t, s->dep_count, s->succ_count, s->succ, s->queue, s->qvalid,
+                   s->blk_done, s->mats_t, s->dep_count, s->succ_count, s->succ, s->queue, s->corners,
                    s->xcounts, s->xblk_base, s->xcoef_base, s->xmeta};
   for (void *p : extra)
     if (p) cudaFree(p);
@@ -312,7 +312,7 @@ extern "C" int mav1cu_session_create(int width, int height, int max_cdef_presets
   if (e == cudaSuccess) e = cudaMalloc(&s->succ_count, sizeof(int) * nblk);
   if (e == cudaSuccess) e = cudaMalloc(&s->succ, sizeof(int) * nblk * MAX_SUCC);
   if (e == cudaSuccess) e = cudaMalloc(&s->queue, sizeof(int) * nblk);
-  if (e == cudaSuccess) e = cudaMalloc(&s->qvalid, sizeof(int) * nblk);
+  if (e == cudaSuccess) e = cudaMalloc(&s->corners, sizeof(int) * nblk);
   s->mats_dirty = 1;
   if (e == cudaSuccess) e = cudaMalloc(&s->blk_list, sizeof(int) * MAX_BLOCKS_PER_SB * nsb);
   if (e == cudaSuccess) e = cudaMalloc(&s->blk_done, 2 * sizeof(int) * MAX_BLOCKS_PER_SB * nsb);
@@ -573,7 +573,7 @@ extern "C" int mav1cu_recon(mav1cu_session *s) {
   if (after_launch(s, "recon claim list")) return s->err;
   size_t nblk = (size_t)MAX_BLOCKS_PER_SB * nsb;
   if (check_cuda(s, cudaMemsetAsync(s->succ_count, 0, sizeof(int) * nblk, s->stream), "recon successors") ||
-      check_cuda(s, cudaMemsetAsync(s->qvalid, 0, sizeof(int) * nblk, s->stream), "recon queue") ||
+      check_cuda(s, cudaMemsetAsync(s->queue, 0, sizeof(int) * nblk, s->stream), "recon queue") ||
       check_cuda(s, cudaMemsetAsync(s->status + 2, 0, sizeof(int), s->stream), "recon queue head") ||
       check_cuda(s, cudaMemsetAsync(s->status + 4, 0, sizeof(int), s->stream), "recon queue tail"))
     return s->err;
@@ -581,7 +581,7 @@ extern "C" int mav1cu_recon(mav1cu_session *s) {
   c.succ_count = s->succ_count;
   c.succ = s->succ;
   c.queue = s->queue;
-  c.qvalid = s->qvalid;
+  c.corners = s->corners;
   c.qtail = s->status + 4;
   rec::k_block_deps<<<(unsigned)imin((int)((nblk + 3) / 4), 4 * s->resident_recon), 128, 0, s->stream>>>(
       c, s->blk_list, s->status + 3);
