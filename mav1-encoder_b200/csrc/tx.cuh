@@ -29,13 +29,22 @@ HD int cos128(int angle) {
 HD int sin128(int angle) { return cos128(angle - 64); }
 
 // Butterfly rotation B( a, b, angle, flip ) (spec 7.13.2.1). T_ is an
-// int32_t pointer or an Offset view.
+// int32_t pointer or an Offset view. The products and their sums are formed
+// in 32 bits: every input is a 16-bit value (a dequantised level or a row
+// output, both clamped to 16 bits, or an H output clamped to r = 16 bits) or
+// a butterfly output of such values, and the cosines have 12 bits, so the
+// sums stay below 2^30 (tests/native/butterfly_range_check.cpp drives every
+// transform with extreme inputs and checks each sum in 64 bits through
+// MAV1_BUTTERFLY_CHECK).
 template <class T_>
 HD void B(T_ t, int a, int b, int angle, int flip) {
-  int64_t c = cos128(angle), s = sin128(angle);
-  int64_t x = (int64_t)t[a] * c - (int64_t)t[b] * s;
-  int64_t y = (int64_t)t[a] * s + (int64_t)t[b] * c;
-  int32_t xa = (int32_t)round2l(x, 12), yb = (int32_t)round2l(y, 12);
+  int c = cos128(angle), s = sin128(angle);
+  int ta = t[a], tb = t[b];
+#ifdef MAV1_BUTTERFLY_CHECK
+  MAV1_BUTTERFLY_CHECK(ta, tb, c, s);
+#endif
+  int x = ta * c - tb * s, y = ta * s + tb * c;
+  int xa = (x + 2048) >> 12, yb = (y + 2048) >> 12;
   t[a] = flip ? yb : xa;
   t[b] = flip ? xa : yb;
 }

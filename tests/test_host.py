@@ -114,3 +114,20 @@ def test_split_large_inverse_dct_is_exact(tmp_path):
                    check=True, capture_output=True)
     r = subprocess.run([str(exe)], capture_output=True, text=True)
     assert r.returncode == 0, r.stdout + r.stderr
+
+def test_butterfly_sums_fit_32_bits(tmp_path):
+    """Every inverse transform's butterfly sums stay inside 32 bits on
+    extreme 16-bit inputs (tests/native/butterfly_range_check.cpp), so the
+    32-bit tx::B equals the specification's rotation."""
+    import shutil
+    import subprocess
+    cxx = shutil.which("g++")
+    if cxx is None:
+        pytest.skip("no host C++ compiler")
+    exe = tmp_path / "butterfly_range_check"
+    subprocess.run([cxx, "-O2", "-std=c++17", "-I", os.path.join(ROOT, "include"),
+                    "-I", os.path.join(ROOT, "mav1-encoder_b200", "csrc"), "-x", "c++",
+                    os.path.join(ROOT, "tests", "native", "butterfly_range_check.cpp"), "-o", str(exe)],
+                   check=True, capture_output=True)
+    r = subprocess.run([str(exe)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stdout + r.stderr
