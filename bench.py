@@ -232,8 +232,9 @@ def kernel_times(sess, stream, frames_dev):
     kernels are launched on.
 
     dominant: the reconstruction stage of the clip's first key frame, which is
-    the dominant kernel k_recon_blocks (the intra block workers, 29% of the
-    clip's device time in the ncu launch list) plus four short set-up launches.
+    the kernel k_recon_blocks (the intra block workers, 24% of the clip's
+    device time in the ncu launch list, level with the analysis levels) plus
+    four short set-up launches.
     A fresh stream codes the key frame, then the stage is re-run on the engine
     session that holds the frame's analysis output (recon reproduces its
     outputs from the same inputs). stage_ms: every stage of one ALTREF frame,
@@ -296,7 +297,7 @@ def kernel_times(sess, stream, frames_dev):
 KEY_RECON_BYTES = 2 * 3133440 + 2 * 510 * 64 * 108 + 510 * 6144 * 4 + 61440 * 4
 # dram__bytes_read.sum + dram__bytes_write.sum of that launch of k_recon_blocks
 # in one ncu capture (the key frame of `bench.py --profile-frames 3`).
-KEY_RECON_DRAM_BYTES = 15770000
+KEY_RECON_DRAM_BYTES = 19850000
 
 
 def roofline(kern, peaks):
