@@ -10,7 +10,7 @@
 // (analyze_sb_table :697-808).
 //
 // B200 mapping: one warp per candidate block. Each lane predicts whole 4x4
-// units in registers (inter samples through pred::inter_pixel, intra samples
+// units in registers (inter samples through pred::inter_unit4, intra samples
 // from edge arrays in the warp's shared memory), so a prediction is never
 // materialised; SATD sums are reduced with shuffles. Levels run as separate
 // launches 64x64 -> 8x8 because the depth pruning reads the ancestors' costs.
@@ -104,8 +104,9 @@ __device__ int inter_plane_satd(const FrameParams *fp, const uint8_t *src, const
     int ux = (u % nux) * 4, uy = (u / nux) * 4;
     if (usub > 1 && (((uy >> 2) + (ux >> 2)) & 1)) continue;
     int d[16];
+    pred::inter_unit4(&ip, uy, ux, d);
     for (int r = 0; r < 4; r++)
-      for (int c = 0; c < 4; c++) d[r * 4 + c] = (int)sp[(uy + r) * stride + ux + c] - pred::inter_pixel(&ip, uy + r, ux + c);
+      for (int c = 0; c < 4; c++) d[r * 4 + c] = (int)sp[(uy + r) * stride + ux + c] - d[r * 4 + c];
     s += pred::satd4x4(d);
   }
   return gsum(s, g) * usub;
@@ -132,10 +133,12 @@ __device__ void inter3(const FrameParams *fp, const uint8_t *src, const uint8_t 
       int ux = (u % nux) * 4, uy = (u / nux) * 4;
       if (usub > 1 && (((uy >> 2) + (ux >> 2)) & 1)) continue;
       int d0[16], d1[16], d2[16];
+      pred::inter_unit4(&pa, uy, ux, d0);
+      pred::inter_unit4(&pb, uy, ux, d1);
       for (int r = 0; r < 4; r++)
         for (int c = 0; c < 4; c++) {
           int sv = sp[(uy + r) * stride + ux + c];
-          int va = pred::inter_pixel(&pa, uy + r, ux + c), vb = pred::inter_pixel(&pb, uy + r, ux + c);
+          int va = d0[r * 4 + c], vb = d1[r * 4 + c];
           d0[r * 4 + c] = sv - va;
           d1[r * 4 + c] = sv - vb;
           d2[r * 4 + c] = sv - ((va + vb + 1) >> 1);

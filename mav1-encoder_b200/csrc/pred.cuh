@@ -26,6 +26,7 @@ struct Inter {
   const uint8_t *ref;  // plane origin
   int stride, lastX, lastY;
   int ix0, iy0;        // integer position of output sample (0, 0) minus 3
+  int fullpel;         // both filter positions 0: every filter is the identity there
   int16_t fh[8], fv[8];  // taps span -128..128
 };
 
@@ -40,6 +41,7 @@ HD void inter_setup(Inter *p, const uint8_t *ref, int stride, int refW, int refH
   p->lastY = ((refH + subY) >> subY) - 1;
   p->ix0 = (px >> 4) - 3;
   p->iy0 = (py >> 4) - 3;
+  p->fullpel = ((px | py) & 15) == 0;
   int fv = filter & 3, fh = (filter >> 2) & 3;
   if (w <= 4) fh = (fh == EIGHTTAP || fh == EIGHTTAP_SHARP) ? 4 : (fh == EIGHTTAP_SMOOTH ? 5 : fh);
   if (h <= 4) fv = (fv == EIGHTTAP || fv == EIGHTTAP_SHARP) ? 4 : (fv == EIGHTTAP_SMOOTH ? 5 : fv);
@@ -68,6 +70,41 @@ HD int inter_sum(const Inter *p, int r, int c) {
 HD int inter_pixel(const Inter *p, int r, int c) { return clip1(round2(inter_sum(p, r, c), 11)); }
 // Compound intermediate (isCompound: InterRound1 = 7, not clipped).
 HD int inter_raw(const Inter *p, int r, int c) { return round2(inter_sum(p, r, c), 7); }
+
+// The 16 single-reference samples of the 4x4 unit at (r0, c0), row-major
+// into o: inter_pixel in separable form. A horizontal sum Round2( ., 3 )
+// depends only on its row and column, so the unit's 11 x 4 of them are
+// formed once (11 x 11 reference samples) and each output takes 8 of them;
+// at a full-sample position every filter is (0, 0, 0, 128, 0, 0, 0, 0) and
+// the prediction is the clamped reference sample itself.
+HD void inter_unit4(const Inter *p, int r0, int c0, int *o) {
+  if (p->fullpel) {
+    for (int r = 0; r < 4; r++) {
+      const uint8_t *row = p->ref + (size_t)clip3(0, p->lastY, p->iy0 + 3 + r0 + r) * p->stride;
+      for (int c = 0; c < 4; c++) o[r * 4 + c] = row[clip3(0, p->lastX, p->ix0 + 3 + c0 + c)];
+    }
+    return;
+  }
+  int xs[11];
+  for (int t = 0; t < 11; t++) xs[t] = clip3(0, p->lastX, p->ix0 + c0 + t);
+  int hs[11][4];
+  for (int tv = 0; tv < 11; tv++) {
+    const uint8_t *row = p->ref + (size_t)clip3(0, p->lastY, p->iy0 + r0 + tv) * p->stride;
+    int px[11];
+    for (int t = 0; t < 11; t++) px[t] = row[xs[t]];
+    for (int c = 0; c < 4; c++) {
+      int s = 0;
+      for (int t = 0; t < 8; t++) s += p->fh[t] * px[c + t];
+      hs[tv][c] = round2(s, 3);
+    }
+  }
+  for (int r = 0; r < 4; r++)
+    for (int c = 0; c < 4; c++) {
+      int acc = 0;
+      for (int tv = 0; tv < 8; tv++) acc += p->fv[tv] * hs[r + tv][c];
+      o[r * 4 + c] = clip1(round2(acc, 11));
+    }
+}
 
 // ---- SATD --------------------------------------------------------------------
 // 4x4 Hadamard SATD of a difference block d[row * 4 + col] (the analysis
