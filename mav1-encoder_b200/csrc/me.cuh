@@ -223,6 +223,16 @@ __device__ int unit_satd_hp(const Frame &f, const Node &m, int mvr, int mvc, int
   int iy = uy + (mvr >> 3), ix = ux + (mvc >> 3);
   const uint8_t *sp = f.src + fp->offset[0] + uy * fp->stride[0] + ux;
   int d[16];
+  if (ix >= 0 && ix + 8 <= W && iy >= 0 && iy + 4 <= H) {
+    // inside the plane, and the two aligned words each row load stay in the
+    // row: no clamping; the source row is word aligned (ux % 4 == 0)
+    for (int r = 0; r < 4; r++) {
+      uint32_t pv = load_u32_unaligned(pl + (size_t)(iy + r) * W + ix);
+      uint32_t sv = __ldg((const uint32_t *)(sp + r * fp->stride[0]));
+      for (int c = 0; c < 4; c++) d[r * 4 + c] = (int)((sv >> (8 * c)) & 255) - (int)((pv >> (8 * c)) & 255);
+    }
+    return pred::satd4x4(d);
+  }
   for (int r = 0; r < 4; r++) {
     const uint8_t *row = pl + (size_t)clip3(0, H - 1, iy + r) * W;
     for (int c = 0; c < 4; c++) d[r * 4 + c] = (int)sp[r * fp->stride[0] + c] - (int)row[clip3(0, W - 1, ix + c)];
