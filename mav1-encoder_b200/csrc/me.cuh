@@ -255,28 +255,32 @@ __device__ int unit_satd_pred(const Frame &f, const Node &m, int mvr, int mvc, i
   return pred::satd4x4(d);
 }
 
-__device__ __forceinline__ unsigned long long warp_min_u64(unsigned long long v) {
-  for (int off = 16; off > 0; off >>= 1) {
-    unsigned long long o = __shfl_xor_sync(0xffffffffu, v, off);
-    v = o < v ? o : v;
-  }
-  return v;
-}
-
 __device__ __forceinline__ void sub_neighbour(const FrameParams *fp, int j, int step, int *dr, int *dc) {
   int k = (fp->turbo & T_ME_CROSS) ? (j == 0 ? 1 : j == 1 ? 3 : j == 2 ? 4 : 6) : j;
   *dr = (k < 3) ? -step : (k < 5 ? 0 : step);
   *dc = (k == 0 || k == 3 || k == 5) ? -step : ((k == 1 || k == 6) ? 0 : step);
 }
 
-// The threads searching one node: a warp, or for the 64x64 level the CTA.
+// The threads searching one node: the CTA (the 64x64 level), a warp, or
+// half a warp (the 8x8 level, whose nodes have at most 16 sub-pel pairs at
+// a time); mask holds the group's lanes of its warp.
 struct MeGrp {
   int rank, size;
+  unsigned mask;
   __device__ __forceinline__ void sync() const {
-    if (size == 32) __syncwarp();
-    else __syncthreads();
+    if (size > 32) __syncthreads();
+    else __syncwarp(mask);
   }
 };
+
+// Minimum over the group's lanes of its warp (the whole warp for a CTA group).
+__device__ __forceinline__ unsigned long long group_min(unsigned long long v, const MeGrp &g) {
+  for (int off = g.size >= 32 ? 16 : g.size >> 1; off > 0; off >>= 1) {
+    unsigned long long o = __shfl_xor_sync(g.mask, v, off);
+    v = o < v ? o : v;
+  }
+  return v;
+}
 
 // Sub-pel costs of ncand candidates (mvr[c], mvc[c]) into cost[c] (shared,
 // private to the group), every (candidate, unit) pair spread over the group.
@@ -299,20 +303,23 @@ __device__ void subpel_costs(const Frame &f, const Node &m, const int *cr, const
   g.sync();
 }
 
-// One search level: warp per (node, reference), or with whole_cta the
-// CTA's four warps per node (the 64x64 level: few, large nodes);
-// blockIdx.y selects the reference.
-__global__ void __launch_bounds__(128) k_me_level(Frame f0, Frame f1, int level, int whole_cta) {
-  __shared__ int s_cost[4][16];
-  __shared__ int s_r[4][16], s_c[4][16];
+// One search level: with group 128 the CTA's four warps per node (the 64x64
+// level: few, large nodes), with 32 a warp per (node, reference), with 16
+// half a warp (the 8x8 level); blockIdx.y selects the reference.
+__global__ void __launch_bounds__(128) k_me_level(Frame f0, Frame f1, int level, int group) {
+  __shared__ int s_cost[8][16];
+  __shared__ int s_r[8][16], s_c[8][16];
   __shared__ unsigned long long s_best[4];
   const Frame &f = blockIdx.y ? f1 : f0;
   const FrameParams *fp = f.fp;
   int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  MeGrp grp = whole_cta ? MeGrp{(int)threadIdx.x, 128} : MeGrp{lane, 32};
-  int slotw = whole_cta ? 0 : warp;
+  int whole_cta = group == 128, half = lane >> 4;
+  MeGrp grp = whole_cta ? MeGrp{(int)threadIdx.x, 128, 0xffffffffu}
+              : group == 32 ? MeGrp{lane, 32, 0xffffffffu}
+                            : MeGrp{lane & 15, 16, 0xffffu << (16 * half)};
+  int slotw = whole_cta ? 0 : group == 32 ? warp : 2 * warp + half;
   int nn = 1 << (2 * level);
-  int g = whole_cta ? (int)blockIdx.x : (int)blockIdx.x * 4 + warp;
+  int g = whole_cta ? (int)blockIdx.x : (int)blockIdx.x * (128 / group) + slotw;
   if (g >= fp->sb_cols * fp->sb_rows * nn) return;
   int sb = g / nn, i = g % nn;
   Node m = make_node(fp, sb, level, i, f.mv);
@@ -339,7 +346,7 @@ __global__ void __launch_bounds__(128) k_me_level(Frame f0, Frame f1, int level,
       unsigned long long key = ((unsigned long long)(unsigned)full_cost(f, m, dy, dx) << 32) | (unsigned)k;
       best = key < best ? key : best;
     }
-    best = warp_min_u64(best);
+    best = group_min(best, grp);
     if (whole_cta) {
       __syncthreads();
       if (lane == 0) s_best[warp] = best;

@@ -485,9 +485,11 @@ extern "C" int mav1cu_motion_search(mav1cu_session *s) {
   }
   for (int level = 0; level < 4; level++) {
     int nodes = s->g.num_sbs << (2 * level);
-    int whole = level == 0;  // the 64x64 nodes: one CTA each
-    dim3 grid(whole ? nodes : (nodes + 3) / 4, nref);
-    me::k_me_level<<<grid, 128, 0, s->stream>>>(f[0], f[1], level, whole);
+    // threads per node: the CTA for the 64x64 nodes, half a warp for the 8x8
+    // nodes, a warp otherwise
+    int group = level == 0 ? 128 : level == 3 ? 16 : 32;
+    dim3 grid((nodes + 128 / group - 1) / (128 / group), nref);
+    me::k_me_level<<<grid, 128, 0, s->stream>>>(f[0], f[1], level, group);
     if (after_launch(s, "motion search")) return s->err;
   }
   return MAV1CU_OK;
