@@ -48,18 +48,24 @@ __device__ __forceinline__ long long warp_sum64(long long v) {
   return v;
 }
 
-// The threads evaluating one candidate: a warp (rank = lane), or for the
-// 64x64 level a whole CTA (red: one shared word per warp). Sums are the
-// warp sums, then across the CTA's warps.
+// The threads evaluating one candidate: a warp (rank = lane), half a warp
+// (the 8x8 level: a few 4x4 units per candidate; mask holds its lanes), or
+// for the 64x64 level a whole CTA (red: one shared word per warp). Sums are
+// the group's lanes' sums, then across the CTA's warps.
 struct Grp {
   int rank, size;
   long long *red;
+  unsigned mask;
 };
 __device__ __forceinline__ void gsync(const Grp &g) {
-  if (g.size == 32) __syncwarp();
+  if (g.size <= 32) __syncwarp(g.mask);
   else __syncthreads();
 }
 __device__ __forceinline__ long long gsum64(long long v, const Grp &g) {
+  if (g.size < 32) {
+    for (int off = g.size >> 1; off > 0; off >>= 1) v += __shfl_xor_sync(g.mask, v, off);
+    return v;
+  }
   v = warp_sum64(v);
   if (g.size == 32) return v;
   __syncthreads();
@@ -528,16 +534,23 @@ __device__ int depth_pruned(const FrameParams *fp, const int64_t *costs, int sbI
 // whole_cta the CTA's four warps on one item (the 64x64 level, whose few
 // large items would otherwise leave most SMs idle).
 #define ANA_THREADS 128
-__global__ void __launch_bounds__(ANA_THREADS) k_analyze_level(Ctx c, int level, int slots, int whole_cta) {
+// group: threads per candidate (ANA_THREADS, 32 or 16; ana_groups gives the
+// edge scratch areas the dynamic shared memory holds).
+__host__ __device__ constexpr int ana_groups(int group) { return group < 32 ? ANA_THREADS / group : ANA_THREADS / 32; }
+__global__ void __launch_bounds__(ANA_THREADS) k_analyze_level(Ctx c, int level, int slots, int group) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   WarpMem *wmem = (WarpMem *)smem_raw;
-  long long *red = (long long *)(wmem + ANA_THREADS / 32);
+  long long *red = (long long *)(wmem + ana_groups(group));
   const FrameParams *fp = c.fp;
-  int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, half = lane >> 4;
+  int whole_cta = group == ANA_THREADS;
+  int gi = whole_cta ? 0 : group == 32 ? warp : 2 * warp + half;
   int n = 1 << level, per = n * n * slots;
-  int item = whole_cta ? (int)blockIdx.x : (int)blockIdx.x * (ANA_THREADS / 32) + warp;
-  Grp grp = whole_cta ? Grp{(int)threadIdx.x, ANA_THREADS, red} : Grp{lane, 32, nullptr};
-  WarpMem &wm = wmem[whole_cta ? 0 : warp];
+  int item = whole_cta ? (int)blockIdx.x : (int)blockIdx.x * (ANA_THREADS / group) + gi;
+  Grp grp = whole_cta ? Grp{(int)threadIdx.x, ANA_THREADS, red, 0xffffffffu}
+            : group == 32 ? Grp{lane, 32, nullptr, 0xffffffffu}
+                          : Grp{lane & 15, 16, nullptr, 0xffffu << (16 * half)};
+  WarpMem &wm = wmem[gi];
   if (item >= fp->sb_cols * fp->sb_rows * per) return;
   int sbIdx = item / per, rem = item % per, i = rem / slots, slot = rem % slots;
   int sbRow = sbIdx / fp->sb_cols, sbCol = sbIdx % fp->sb_cols;

@@ -24,9 +24,10 @@
 #include "stream.cuh"
 #include "export.cuh"
 
-// dynamic shared memory of the analysis pass-1 kernel: a WarpMem per warp
+// dynamic shared memory of the analysis pass-1 kernel for candidate groups of
+// `group` threads: a WarpMem (edge scratch) per group (per warp for CTA groups)
 // and one reduction word per warp
-#define ANA_SMEM (ANA_THREADS / 32 * sizeof(ana::WarpMem) + ANA_THREADS / 32 * sizeof(long long))
+#define ANA_SMEM(group) (ana::ana_groups(group) * sizeof(ana::WarpMem) + ANA_THREADS / 32 * sizeof(long long))
 
 namespace {
 
@@ -353,7 +354,7 @@ extern "C" int mav1cu_session_create(int width, int height, int max_cdef_presets
     // rest of each SM stays free for the other engines' kernels
     s->resident_recon = imax(1, sms * imin(1, imax(1, per)));
   }
-  cudaFuncSetAttribute(ana::k_analyze_level, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ANA_SMEM);
+  cudaFuncSetAttribute(ana::k_analyze_level, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ANA_SMEM(16));
   *out = s;
   return MAV1CU_OK;
 }
@@ -517,9 +518,10 @@ extern "C" int mav1cu_analyze(mav1cu_session *s) {
   for (int level = 0; level < 4; level++) {
     int slots = ana::level_slots(&s->fp, level);
     long long items = (long long)s->g.num_sbs * (1 << (2 * level)) * slots;
-    int whole = level == 0;  // the 64x64 candidates: one CTA each
-    unsigned grid = (unsigned)(whole ? items : (items + ANA_THREADS / 32 - 1) / (ANA_THREADS / 32));
-    ana::k_analyze_level<<<grid, ANA_THREADS, ANA_SMEM, s->stream>>>(c, level, slots, whole);
+    // threads per candidate: the CTA for 64x64, half a warp for 8x8, a warp otherwise
+    int group = level == 0 ? ANA_THREADS : level == 3 ? 16 : 32, per = ANA_THREADS / group;
+    unsigned grid = (unsigned)((items + per - 1) / per);
+    ana::k_analyze_level<<<grid, ANA_THREADS, ANA_SMEM(group), s->stream>>>(c, level, slots, group);
     if (after_launch(s, "analysis pass 1")) return s->err;
   }
   ana::k_analyze_table<<<(s->g.num_sbs + TABLE_WARPS - 1) / TABLE_WARPS, 32 * TABLE_WARPS, 0, s->stream>>>(c);
