@@ -518,8 +518,9 @@ extern "C" int mav1cu_analyze(mav1cu_session *s) {
   for (int level = 0; level < 4; level++) {
     int slots = ana::level_slots(&s->fp, level);
     long long items = (long long)s->g.num_sbs * (1 << (2 * level)) * slots;
-    // threads per candidate: the CTA for 64x64, half a warp for 8x8, a warp otherwise
-    int group = level == 0 ? ANA_THREADS : level == 3 ? 16 : 32, per = ANA_THREADS / group;
+    // threads per candidate: the CTA for 64x64, a warp for 32x32, half a warp
+    // for 16x16 and 8x8 (at most 16 luma 4x4 units per candidate)
+    int group = level == 0 ? ANA_THREADS : level >= 2 ? 16 : 32, per = ANA_THREADS / group;
     unsigned grid = (unsigned)((items + per - 1) / per);
     ana::k_analyze_level<<<grid, ANA_THREADS, ANA_SMEM(group), s->stream>>>(c, level, slots, group);
     if (after_launch(s, "analysis pass 1")) return s->err;
