@@ -232,9 +232,9 @@ def kernel_times(sess, stream, frames_dev):
     kernels are launched on.
 
     dominant: the reconstruction stage of the clip's first key frame, which is
-    the kernel k_recon_blocks (the intra block workers, 24% of the clip's
-    device time in the ncu launch list, level with the analysis levels) plus
-    four short set-up launches.
+    the dominant kernel k_recon_blocks (the intra block workers, 28% of the
+    clip's device time in the ncu launch list) plus four short set-up
+    launches.
     A fresh stream codes the key frame, then the stage is re-run on the engine
     session that holds the frame's analysis output (recon reproduces its
     outputs from the same inputs). stage_ms: every stage of one ALTREF frame,
