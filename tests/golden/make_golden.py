@@ -49,7 +49,53 @@ def run(name):
     }
 
 
+# Full-size cases, too slow for the oracle inside a test (minutes of CPU
+# per 4K frame with every tool on): their hashes are checked against the
+# CUDA backend through the drop-in (tests/test_dropin_gpu.py). Written to
+# dropin_hashes.json by `make_golden.py --large`.
+LARGE_CASES = {
+    # the benchmark spec's full-tool configuration (3840x2160, -q 90, tx
+    # search, tx depth, switchable / dual filter, CDEF, loop restoration,
+    # --altref 16 --golden --tiles 3, ME range 64): its first 3 frames
+    "c2_2160p_full_3f": ("c2_2160p", 3, dict(q=90, altref=16, golden=1, tiles=3, me_range=64)),
+}
+
+
+def large_frames(name):
+    clip, n, flags = LARGE_CASES[name]
+    spec = synthetic.CONFIGS[clip]
+    return spec, list(synthetic.generate(spec, n)), flags
+
+
+def frames_sha256(frames):
+    return hashlib.sha256(b"".join(synthetic.packed(f) for f in frames)).hexdigest()
+
+
+def run_large(name):
+    spec, frames, flags = large_frames(name)
+    with tempfile.TemporaryDirectory() as d:
+        dump = os.path.join(d, "dec")
+        os.environ["MAV1_DUMP_DEC"] = dump
+        try:
+            packets, recons = oracle.encode(frames, oracle.cli_config(spec.width, spec.height, **flags))
+        finally:
+            del os.environ["MAV1_DUMP_DEC"]
+        dec = open(dump, "rb").read()
+    h = lambda b: hashlib.sha256(b).hexdigest()
+    return {
+        "frames": frames_sha256(frames),
+        "ivf": h(oracle.ivf_bytes(packets, spec.width, spec.height)),
+        "recon": h(b"".join(p.tobytes() for r in recons for p in r)),
+        "dump": h(dec),
+        "packets": len(packets),
+    }
+
+
 if __name__ == "__main__":
-    out = {name: run(name) for name in CASES}
-    json.dump(out, open(os.path.join(HERE, "oracle_hashes.json"), "w"), indent=1, sort_keys=True)
+    if "--large" in sys.argv:
+        out = {name: run_large(name) for name in LARGE_CASES}
+        json.dump(out, open(os.path.join(HERE, "dropin_hashes.json"), "w"), indent=1, sort_keys=True)
+    else:
+        out = {name: run(name) for name in CASES}
+        json.dump(out, open(os.path.join(HERE, "oracle_hashes.json"), "w"), indent=1, sort_keys=True)
     print(json.dumps(out, indent=1))

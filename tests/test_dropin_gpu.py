@@ -53,3 +53,33 @@ def test_dropin_bitstream_identical(name, tmp_path):
         for pa, pb in zip(a, b):
             assert np.array_equal(pa, pb)
     assert (tmp_path / "cpu.dec").read_bytes() == (tmp_path / "cuda.dec").read_bytes()
+
+
+@pytest.mark.skipif(not (oracle.available() and oracle.available(oracle.HYB_PATH)), reason="oracle not built")
+def test_dropin_full_tools_2160p_matches_golden(tmp_path):
+    """The benchmark spec's full-tool configuration at full size (3840x2160,
+    -q 90, tx search, tx depth, switchable / dual filter, CDEF, loop
+    restoration, --altref 16 --golden --tiles 3, ME range 64; its first 3
+    frames) through the drop-in, against SHA-256 hashes of the oracle's IVF
+    bitstream, reconstructions and decision dump for the same frames
+    (tests/golden/dropin_hashes.json, written by tests/golden/make_golden.py
+    --large: the oracle needs minutes per frame at this size)."""
+    import hashlib
+    import importlib.util
+    import json
+    here = os.path.dirname(os.path.abspath(__file__))
+    spec_ = importlib.util.spec_from_file_location("make_golden", os.path.join(here, "golden", "make_golden.py"))
+    mg = importlib.util.module_from_spec(spec_)
+    spec_.loader.exec_module(mg)
+    name = "c2_2160p_full_3f"
+    want = json.load(open(os.path.join(here, "golden", "dropin_hashes.json")))[name]
+    spec, frames, flags = mg.large_frames(name)
+    assert mg.frames_sha256(frames) == want["frames"]
+    dump = str(tmp_path / "cuda.dec")
+    packets, recons = _encode(spec, len(frames), flags, True, dump)
+    h = lambda b: hashlib.sha256(b).hexdigest()
+    assert len(packets) == want["packets"]
+    assert h(oracle.ivf_bytes(packets, spec.width, spec.height)) == want["ivf"]
+    assert h(b"".join(p.tobytes() for r in recons for p in r)) == want["recon"]
+    assert h(open(dump, "rb").read()) == want["dump"]
+
