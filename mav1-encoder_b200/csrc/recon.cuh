@@ -92,7 +92,7 @@ struct Smem {
   int32_t q[32 * 32];      // levels of the current candidate
   int32_t qbest[32 * 32];  // levels kept by the tx type search
   int sse33[33];
-  long long red[INTER_THREADS / 32];
+  long long red[(INTER_THREADS > INTRA_THREADS ? INTER_THREADS : INTRA_THREADS) / 32];  // one per warp
   BlockInfo blk;
   int maxLumaW, maxLumaH;
   int flag;
