@@ -1415,9 +1415,10 @@ struct Claim {
   int *next;
 };
 
-// Every block of the frame, one persistent launch: each CTA (one warp)
-// claims the next block of the list, codes it (waiting inside on the blocks
-// its intra edges read) and publishes its completion flag.
+// Every intra block of the frame, one persistent launch: each worker CTA
+// takes the next slot of the ready queue, waits (bounded) until a released
+// block fills it, stages and codes that block (its luma, published with its
+// successors released, then its chroma) and publishes its completion flags.
 __global__ void __launch_bounds__(INTRA_THREADS, 1) k_recon_blocks(Ctx cg, Claim q) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   // workers in proportion to the frame's intra blocks: the surplus CTAs

@@ -350,8 +350,9 @@ extern "C" int mav1cu_session_create(int width, int height, int max_cdef_presets
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, rec::k_recon_blocks, rec::INTRA_THREADS, rec::SMEM_INTRA);
-    // one worker per SM: the ready queue keeps them on ready blocks, and the
-    // rest of each SM stays free for the other engines' kernels
+    // at most one worker per SM (the kernel keeps max(8, intra blocks / 8) of
+    // them): the ready queue keeps them on ready blocks, and the rest of each
+    // SM stays free for the other engines' kernels
     s->resident_recon = imax(1, sms * imin(1, imax(1, per)));
   }
   cudaFuncSetAttribute(ana::k_analyze_level, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ANA_SMEM(16));
