@@ -118,6 +118,18 @@ def split_gops(jobs):
     return gops
 
 
+def max_over_ranks(values, device):
+    """Element-wise maximum of this rank's timings over the process group:
+    each replica times its own GPU, and the slowest one defines the step. The
+    only collectives of a multi-GPU run are this and the barriers around the
+    timed region (the replicas share no data)."""
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor(values, dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return t.tolist()
+
+
 def run_ours(args, rank, world):
     import torch
     import mav1cu
@@ -216,10 +228,7 @@ def run_ours(args, rank, world):
     per_e2e = sum(ms_e2e) / len(ms_e2e)
     per_seq = sum(ms_seq) / len(ms_seq)
     if world > 1:
-        import torch.distributed as dist
-        t = torch.tensor([per_step, per_e2e, per_seq], dtype=torch.float64, device=f"cuda:{dev}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        per_step, per_e2e, per_seq = t.tolist()
+        per_step, per_e2e, per_seq = max_over_ranks([per_step, per_e2e, per_seq], f"cuda:{dev}")
     kern = kernel_times(streams[0].session, S, frames_dev) if (rank == 0 and not args.no_roofline) else None
     for st in streams:
         st.close()
