@@ -253,6 +253,43 @@ typedef struct {
  * of a clip of nframes frames into jobs (at most cap). Returns the number of
  * jobs, or a negative status. */
 int mav1cu_plan(const mav1cu_config *cfg, int nframes, mav1cu_frame_job *jobs, int cap);
+/* Incremental planning for a caller that receives frames one at a time (the
+ * queue API mav1_send_frame, encoder.c:1295-1320): the state of the
+ * reference driver's frame queue between calls. Zero-initialise it before the
+ * first call. */
+typedef struct {
+  int32_t in_disp;        /* frames received so far */
+  int32_t inq_n;          /* received frames not yet planned (ALTREF driver) */
+  int32_t key_disp;       /* display index of the last key frame */
+  int32_t anchor_slot;    /* slot of the last shown reference frame */
+  int32_t ld_order_hint;  /* low-delay driver: OrderHint of the next frame */
+  int32_t ld_last_id, ld_gold_id; /* low-delay driver: frames held by LAST / GOLDEN */
+  int32_t pad[9];
+} mav1cu_planner;
+
+/* Adds new_frames received frames to the queue and writes the jobs that can
+ * now be coded into jobs (coding order, at most cap): with ALTREF a mini-GOP
+ * is planned once all of its frames are queued, or at once when flush is set
+ * (end of stream: alt_drain, encoder.c:1252-1293); without ALTREF every frame
+ * is planned as it arrives (mav1_encode, encoder.c:822-875). Returns the
+ * number of jobs, or a negative status. The jobs of a whole clip equal
+ * mav1cu_plan's, whatever the split into calls. */
+int mav1cu_plan_frames(const mav1cu_config *cfg, mav1cu_planner *state, int new_frames, int flush,
+                       mav1cu_frame_job *jobs, int cap);
+
+/* Normalised configuration and tile geometry of an encoder (create_enc,
+ * encoder.c:69-120): turbo implies fast, ALTREF >= 2 and leaf frames; the
+ * tile columns are clamped to the frame. */
+typedef struct {
+  mav1cu_config cfg;      /* the normalised configuration */
+  int32_t leafopt_cfg;    /* leaf-frame savings (MAV1_LEAFOPT, default 0x3F) */
+  int32_t mi_cols, mi_rows, sb_cols, sb_rows, num_sbs;
+  int32_t tile_cols_log2, tile_cols, tile_w_sb, min_log2_tile_cols, max_log2_tile_cols;
+  int32_t stride[3], offset[3], plane_h[3];
+  int64_t frame_bytes;
+} mav1cu_layout;
+int mav1cu_layout_of(const mav1cu_config *cfg, mav1cu_layout *out);
+
 /* Frame parameters of one planned frame (setup_params, encoder.c:407-510).
  * *num_cdef_presets receives the presets the filter stage writes (0 with
  * CDEF off for the frame). */
@@ -361,6 +398,27 @@ void *mav1cu_export_image(mav1cu_session *s);
  * mav1cu_stream_synchronize / mav1cu_stream_join, which cover the transfer
  * streams); until then the caller must not read or reuse it. */
 int mav1cu_export(mav1cu_session *s, void *image, size_t cap, int flags);
+/* Sequence number of the session's last export (the header's seq field);
+ * 0 before the first. */
+int64_t mav1cu_export_seq(const mav1cu_session *s);
+/* Completion of export number seq of the session, for a host consumer that
+ * reads images while the device moves on: wait blocks the calling thread
+ * (without spinning) until that export's image is complete and returns the
+ * session's status (MAV1CU_ERR_DEVICE when a kernel of the session reported
+ * an error); query returns 1 when it is complete, 0 when not yet, or a
+ * negative status. Any host thread may call them; the thread's current
+ * device is set to the session's. The session remembers the last 64
+ * exports: for an older seq the wait covers a later export (the transfer
+ * stream runs in order). */
+int mav1cu_export_wait(mav1cu_session *s, int64_t seq);
+int mav1cu_export_query(mav1cu_session *s, int64_t seq);
+
+/* Page-locked host memory, mapped into the address space of every device
+ * (cudaHostAlloc, portable and mapped): sources the streams upload
+ * asynchronously and export images. NULL on failure. No counterpart in the
+ * reference (its buffers are shared with the GPU through unified memory). */
+void *mav1cu_host_alloc(size_t bytes);
+void mav1cu_host_free(void *p);
 
 /* ---- host helpers (no device work) --------------------------------------- */
 /* Forward transform matrices (Q20), 15 x 4096 int32: least-squares inverses

@@ -60,6 +60,9 @@ Geometry make_geometry(int w, int h) {
 
 }  // namespace
 
+// exports whose completion a host consumer can wait for individually
+#define XRING 64
+
 struct mav1cu_session {
   Geometry g;
   int max_presets;
@@ -87,6 +90,9 @@ struct mav1cu_session {
   cudaStream_t xs;         // transfer stream the exports run on, forked from `stream`
   cudaEvent_t x_fork, x_done;
   int x_pending;           // an export may still read the session's buffers: writers wait for x_done
+  cudaEvent_t xring[XRING];  // completion of export seq, recorded at xring[seq % XRING] (blocking sync)
+  int device;              // the device the session's memory lives on
+  cudaStream_t ss;         // status reads of host consumers (never waits for the session's other streams)
   std::vector<int> wave_start, wave_len;
   int wave_tile_w;
   FrameParams fp;          // host copy of the current parameters
@@ -261,7 +267,10 @@ static void free_all(mav1cu_session *s) {
   if (s->ximage) cudaFreeHost(s->ximage);
   if (s->x_fork) cudaEventDestroy(s->x_fork);
   if (s->x_done) cudaEventDestroy(s->x_done);
+  for (int i = 0; i < XRING; i++)
+    if (s->xring[i]) cudaEventDestroy(s->xring[i]);
   if (s->xs) cudaStreamDestroy(s->xs);
+  if (s->ss) cudaStreamDestroy(s->ss);
   if (s->own_stream) cudaStreamDestroy(s->own_stream);
 }
 
@@ -325,6 +334,10 @@ extern "C" int mav1cu_session_create(int width, int height, int max_cdef_presets
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->xs, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->x_fork, cudaEventDisableTiming);
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->x_done, cudaEventDisableTiming);
+  for (int i = 0; i < XRING && e == cudaSuccess; i++)
+    e = cudaEventCreateWithFlags(&s->xring[i], cudaEventDisableTiming | cudaEventBlockingSync);
+  if (e == cudaSuccess) e = cudaGetDevice(&s->device);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->ss, cudaStreamNonBlocking);
   if (e != cudaSuccess) {
     snprintf(err, errlen, "device allocation failed: %s", cudaGetErrorString(e));
     free_all(s);
@@ -744,9 +757,51 @@ extern "C" int mav1cu_export(mav1cu_session *s, void *image, size_t cap, int fla
                                                  dimg + layout.rec_off);
     if (after_launch(s, "export reconstruction")) return s->err;
   }
-  if (check_cuda(s, cudaEventRecord(s->x_done, s->xs), "export done")) return s->err;
+  if (check_cuda(s, cudaEventRecord(s->x_done, s->xs), "export done") ||
+      check_cuda(s, cudaEventRecord(s->xring[layout.seq % XRING], s->xs), "export done"))
+    return s->err;
   s->x_pending = 1;
   return MAV1CU_OK;
+}
+
+extern "C" void *mav1cu_host_alloc(size_t bytes) {
+  void *p = NULL;
+  if (cudaHostAlloc(&p, bytes ? bytes : 1, cudaHostAllocMapped | cudaHostAllocPortable) != cudaSuccess) return NULL;
+  return p;
+}
+
+extern "C" void mav1cu_host_free(void *p) {
+  if (p) cudaFreeHost(p);
+}
+
+extern "C" int64_t mav1cu_export_seq(const mav1cu_session *s) { return s->xseq; }
+
+// The device status word of the session (non-zero: a kernel gave up), read
+// on the session's status stream: a copy into pageable host memory returns
+// once it is done, and that stream orders after nothing else.
+static int device_status(mav1cu_session *s) {
+  int st = 0;
+  if (cudaMemcpyAsync(&st, s->status, sizeof st, cudaMemcpyDeviceToHost, s->ss) != cudaSuccess ||
+      cudaStreamSynchronize(s->ss) != cudaSuccess)
+    return MAV1CU_ERR_CUDA;
+  return st ? MAV1CU_ERR_DEVICE : MAV1CU_OK;
+}
+
+extern "C" int mav1cu_export_wait(mav1cu_session *s, int64_t seq) {
+  if (seq <= 0 || seq > s->xseq) return MAV1CU_ERR_ARG;
+  if (cudaSetDevice(s->device) != cudaSuccess) return MAV1CU_ERR_CUDA;
+  if (cudaEventSynchronize(s->xring[seq % XRING]) != cudaSuccess) return MAV1CU_ERR_CUDA;
+  return device_status(s);
+}
+
+extern "C" int mav1cu_export_query(mav1cu_session *s, int64_t seq) {
+  if (seq <= 0 || seq > s->xseq) return MAV1CU_ERR_ARG;
+  if (cudaSetDevice(s->device) != cudaSuccess) return MAV1CU_ERR_CUDA;
+  cudaError_t e = cudaEventQuery(s->xring[seq % XRING]);
+  if (e == cudaErrorNotReady) return 0;
+  if (e != cudaSuccess) return MAV1CU_ERR_CUDA;
+  int st = device_status(s);
+  return st ? st : 1;
 }
 
 
@@ -777,6 +832,52 @@ extern "C" int mav1cu_plan(const mav1cu_config *cfg, int nframes, mav1cu_frame_j
   if (n > cap) return MAV1CU_ERR_ARG;
   for (int i = 0; i < n; i++) jobs[i] = pl.jobs[i];
   return n;
+}
+
+extern "C" int mav1cu_plan_frames(const mav1cu_config *cfg, mav1cu_planner *state, int new_frames, int flush,
+                                  mav1cu_frame_job *jobs, int cap) {
+  if (!cfg || !state || new_frames < 0 || (cap > 0 && !jobs)) return MAV1CU_ERR_ARG;
+  drv::Planner pl;
+  pl.n = drv::normalise(cfg);
+  pl.load(*state);
+  if (pl.n.c.altref > 0) {
+    pl.in_disp += new_frames;
+    pl.inq_n += new_frames;
+    pl.alt_drain(flush != 0);
+  } else {
+    for (int f = 0; f < new_frames; f++) pl.low_delay_frame();
+  }
+  int n = (int)pl.jobs.size();
+  if (n > cap) return MAV1CU_ERR_ARG;  // the state is left unchanged
+  for (int i = 0; i < n; i++) jobs[i] = pl.jobs[i];
+  pl.store(state);
+  return n;
+}
+
+extern "C" int mav1cu_layout_of(const mav1cu_config *cfg, mav1cu_layout *out) {
+  if (!cfg || !out) return MAV1CU_ERR_ARG;
+  drv::Norm n = drv::normalise(cfg);
+  memset(out, 0, sizeof *out);
+  out->cfg = n.c;
+  out->leafopt_cfg = n.leafopt_cfg;
+  out->mi_cols = n.mi_cols;
+  out->mi_rows = n.mi_rows;
+  out->sb_cols = n.sb_cols;
+  out->sb_rows = n.sb_rows;
+  out->num_sbs = n.sb_cols * n.sb_rows;
+  out->tile_cols_log2 = n.tile_cols_log2;
+  out->tile_cols = n.tile_cols;
+  out->tile_w_sb = n.tile_w_sb;
+  out->min_log2_tile_cols = n.min_log2_tile_cols;
+  out->max_log2_tile_cols = n.max_log2_tile_cols;
+  Geometry g = make_geometry(n.c.width, n.c.height);
+  for (int p = 0; p < 3; p++) {
+    out->stride[p] = g.stride[p];
+    out->offset[p] = g.offset[p];
+    out->plane_h[p] = g.plane_h[p];
+  }
+  out->frame_bytes = (int64_t)g.frame_bytes;
+  return MAV1CU_OK;
 }
 
 extern "C" int mav1cu_frame_params_for(const mav1cu_config *cfg, const mav1cu_frame_job *job, mav1cu_frame_params *fp,

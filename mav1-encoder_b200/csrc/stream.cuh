@@ -31,6 +31,7 @@ struct Norm {
   mav1cu_config c;
   int leafopt_cfg;
   int mi_cols, mi_rows, sb_cols, sb_rows, tile_w_sb, tile_cols;
+  int tile_cols_log2, min_log2_tile_cols, max_log2_tile_cols;
 };
 
 static Norm normalise(const mav1cu_config *in) {
@@ -65,6 +66,9 @@ static Norm normalise(const mav1cu_config *in) {
   if (l > maxLog2) l = maxLog2;
   n.tile_w_sb = (n.sb_cols + (1 << l) - 1) >> l;
   n.tile_cols = (n.sb_cols + n.tile_w_sb - 1) / n.tile_w_sb;
+  n.tile_cols_log2 = l;
+  n.min_log2_tile_cols = minLog2;
+  n.max_log2_tile_cols = maxLog2;
   return n;
 }
 
@@ -84,7 +88,12 @@ static int frame_q(const Norm &n, int isKey, int orderHint, int nonref, int kind
 struct Planner {
   Norm n;
   std::vector<mav1cu_frame_job> jobs;
+  // ALTREF driver: display index of the current key frame, the anchor slot,
+  // frames received so far and frames received but not yet coded
   int key_disp = 0, anchor_slot = 0, in_disp = 0, inq_n = 0;
+  // low-delay driver (mav1_encode): OrderHint and the frames held by LAST /
+  // GOLDEN (encoder.c:822-875)
+  int ld_order_hint = 0, ld_last_id = 0, ld_gold_id = 0;
 
   // alt_code's frame-structure part (encoder.c:1004-1030)
   void code(int disp, int isKey, int kind, int lastSlot, int arfSlot, int refresh, int hidden) {
@@ -119,18 +128,20 @@ struct Planner {
     for (int d = a + 1; d < b; d++) code(d, 0, 2, as, bs, 0, 0);
   }
 
-  // alt_drain with every frame queued and the stream flushed (encoder.c:1252-1293)
-  void drain(int nframes) {
+  // alt_drain (encoder.c:1252-1293): codes the queued frames that can be
+  // coded, all of them when flushing
+  void alt_drain(bool flush) {
     int N = n.c.altref;
-    in_disp = nframes;
-    inq_n = nframes;
     const int keyint = n.c.keyint;
     while (inq_n > 0) {
       int d0 = in_disp - inq_n;
       int isKey = d0 == 0 || (keyint > 0 && d0 % keyint == 0);
       int L = isKey ? 1 : N;
       if (!isKey && keyint > 0) L = imin(L, (d0 / keyint + 1) * keyint - d0);
-      if (inq_n < L) L = inq_n;
+      if (inq_n < L) {
+        if (!flush) return;
+        L = inq_n;
+      }
       if (isKey || L == 1) {
         code(d0, isKey, 0, anchor_slot, -1, 0x01, 0);
         anchor_slot = 0;
@@ -151,31 +162,61 @@ struct Planner {
     }
   }
 
-  // mav1_encode's frame structure (encoder.c:822-875): LAST in slot 0, GOLDEN in slot 1
-  void low_delay(int nframes) {
-    int orderHint = 0, lastId = 0, goldId = 0;
-    for (int f = 0; f < nframes; f++) {
-      mav1cu_frame_job j = {};
-      int isKey = f == 0 || (n.c.keyint > 0 && f % n.c.keyint == 0);
-      j.disp = f;
-      j.is_key = isKey;
-      j.nonref = !isKey && n.c.nonref_odd && (orderHint & 1);
-      j.base_q_idx = frame_q(n, isKey, orderHint, j.nonref, 0);
-      if (isKey) orderHint = 0;
-      j.order_hint = orderHint;
-      j.golden_refresh = !isKey && !j.nonref && n.c.multi_ref && orderHint % 4 == 0;
-      j.refresh = isKey ? 0xFF : (j.nonref ? 0x00 : 0x01 | (j.golden_refresh ? 0x02 : 0));
-      j.last_slot = isKey ? -1 : 0;
-      j.arf_slot = isKey || !n.c.multi_ref ? -1 : 1;
-      j.gold_differs = goldId != lastId;
-      j.show_existing = -1;
-      jobs.push_back(j);
-      if (!j.nonref) {
-        lastId = f;
-        if (n.c.multi_ref && (isKey || j.golden_refresh)) goldId = f;
-      }
-      orderHint++;
+  // every frame of a clip queued, then the stream flushed
+  void drain(int nframes) {
+    in_disp = nframes;
+    inq_n = nframes;
+    alt_drain(true);
+  }
+
+  // mav1_encode's frame structure for the next frame (encoder.c:822-875):
+  // LAST in slot 0, GOLDEN in slot 1
+  void low_delay_frame() {
+    mav1cu_frame_job j = {};
+    int f = in_disp++;
+    int isKey = f == 0 || (n.c.keyint > 0 && f % n.c.keyint == 0);
+    j.disp = f;
+    j.is_key = isKey;
+    j.nonref = !isKey && n.c.nonref_odd && (ld_order_hint & 1);
+    j.base_q_idx = frame_q(n, isKey, ld_order_hint, j.nonref, 0);
+    if (isKey) ld_order_hint = 0;
+    j.order_hint = ld_order_hint;
+    j.golden_refresh = !isKey && !j.nonref && n.c.multi_ref && ld_order_hint % 4 == 0;
+    j.refresh = isKey ? 0xFF : (j.nonref ? 0x00 : 0x01 | (j.golden_refresh ? 0x02 : 0));
+    j.last_slot = isKey ? -1 : 0;
+    j.arf_slot = isKey || !n.c.multi_ref ? -1 : 1;
+    j.gold_differs = ld_gold_id != ld_last_id;
+    j.show_existing = -1;
+    jobs.push_back(j);
+    if (!j.nonref) {
+      ld_last_id = f;
+      if (n.c.multi_ref && (isKey || j.golden_refresh)) ld_gold_id = f;
     }
+    ld_order_hint++;
+  }
+
+  void low_delay(int nframes) {
+    for (int f = 0; f < nframes; f++) low_delay_frame();
+  }
+
+  // the caller-held state of an incremental plan (mav1cu_planner)
+  void load(const mav1cu_planner &p) {
+    key_disp = p.key_disp;
+    anchor_slot = p.anchor_slot;
+    in_disp = p.in_disp;
+    inq_n = p.inq_n;
+    ld_order_hint = p.ld_order_hint;
+    ld_last_id = p.ld_last_id;
+    ld_gold_id = p.ld_gold_id;
+  }
+  void store(mav1cu_planner *p) const {
+    p->key_disp = key_disp;
+    p->anchor_slot = anchor_slot;
+    p->in_disp = in_disp;
+    p->inq_n = inq_n;
+    p->ld_order_hint = ld_order_hint;
+    p->ld_last_id = ld_last_id;
+    p->ld_gold_id = ld_gold_id;
   }
 };
 

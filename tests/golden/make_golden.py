@@ -24,6 +24,9 @@ CASES = {
     "lowdelay_lr_150x102": (dict(width=150, height=102, frames=6, seed=42, rects=2, rect_size=(16, 40)),
                             dict(q=200, golden=1, keyint=4, lr_test=1)),
     "lossless_96x64": (dict(width=96, height=64, frames=3, seed=43, rects=1, rect_size=(16, 32)), dict(q=0, fast=1)),
+    # the benchmark workload: the whole 120-frame 1080p clip with its flags
+    "c1_1080p_turbo_120": (dict(width=1920, height=1080, frames=120, seed=1, pan=(2.5, 1.0), rects=12,
+                                rect_size=(64, 256)), dict(q=125, turbo=1, keyint=60, tiles=2)),
 }
 
 
@@ -46,6 +49,10 @@ def run(name):
         "recon": h(b"".join(p.tobytes() for r in recons for p in r)),
         "dump": h(dec),
         "packets": len(packets),
+        # per temporal unit: the first 16 hex digits of the SHA-256 of its
+        # bytes and of its shown reconstruction (locates a difference)
+        "packet_sha16": [h(p)[:16] for p in packets],
+        "recon_sha16": [h(b"".join(p.tobytes() for p in r))[:16] for r in recons],
     }
 
 
@@ -96,6 +103,10 @@ if __name__ == "__main__":
         out = {name: run_large(name) for name in LARGE_CASES}
         json.dump(out, open(os.path.join(HERE, "dropin_hashes.json"), "w"), indent=1, sort_keys=True)
     else:
-        out = {name: run(name) for name in CASES}
-        json.dump(out, open(os.path.join(HERE, "oracle_hashes.json"), "w"), indent=1, sort_keys=True)
+        # --case NAME recomputes one entry and keeps the others
+        names = [sys.argv[sys.argv.index("--case") + 1]] if "--case" in sys.argv else list(CASES)
+        path = os.path.join(HERE, "oracle_hashes.json")
+        out = json.load(open(path)) if os.path.exists(path) and "--case" in sys.argv else {}
+        out.update({name: run(name) for name in names})
+        json.dump(out, open(path, "w"), indent=1, sort_keys=True)
     print(json.dumps(out, indent=1))

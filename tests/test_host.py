@@ -64,13 +64,16 @@ def test_spec_table_digest():
     assert h.hexdigest() == digest
 
 
-@pytest.mark.skipif(not os.path.isdir("/root/reference/src"), reason="reference checkout absent")
+REFERENCE = os.environ.get("MAV1_REFERENCE", "/root/reference")
+
+
+@pytest.mark.skipif(not os.path.isdir(os.path.join(REFERENCE, "src")), reason="reference checkout absent")
 def test_spec_tables_regenerate_identically(tmp_path):
     import subprocess
     import sys
     gen = os.path.join(ROOT, "mav1-encoder_b200", "csrc", "gen_spec_tables.py")
     out = tmp_path / "t.h"
-    subprocess.run([sys.executable, gen, "/root/reference/src", str(out)], check=True, capture_output=True)
+    subprocess.run([sys.executable, gen, os.path.join(REFERENCE, "src"), str(out)], check=True, capture_output=True)
     assert out.read_bytes() == open(os.path.join(ROOT, "mav1-encoder_b200", "csrc", "spec_tables_gen.h"), "rb").read()
 
 

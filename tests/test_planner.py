@@ -33,3 +33,35 @@ def test_frame_params_match_oracle(case):
         fp, _ = mav1cu.frame_params(cfg, job)
         ref = parity.params_of(fr)
         assert np.array_equal(fp, ref), (k, job, np.flatnonzero(fp.view(np.int32) != ref.view(np.int32)))
+
+
+PLANNER_DTYPE = np.dtype([(n, "<i4") for n in ["in_disp", "inq_n", "key_disp", "anchor_slot", "ld_order_hint",
+                                                 "ld_last_id", "ld_gold_id"]] + [("pad", "<i4", (9,))])
+
+
+@pytest.mark.parametrize("flags,n", [(dict(turbo=1, keyint=60), 120), (dict(altref=8, leaf=1), 37),
+                                     (dict(altref=4, golden=1), 23), (dict(golden=1, keyint=4), 11),
+                                     (dict(turbo=1, keyint=8), 9), (dict(altref=16, golden=1), 32),
+                                     (dict(q=90, nonref=1), 10)])
+def test_incremental_plan_equals_whole_clip(flags, n):
+    """mav1cu_plan_frames fed one frame at a time, then flushed (the queue
+    API's mav1_send_frame sequence), plans the same jobs in the same order as
+    mav1cu_plan over the whole clip."""
+    import ctypes
+    L = mav1cu.lib()
+    L.mav1cu_plan_frames.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
+                                     ctypes.c_int]
+    nonref = flags.pop("nonref", 0)
+    cfg = mav1cu.cli_config(352, 288, **flags)
+    cfg[0]["nonref_odd"] = nonref
+    whole = [tuple(j) for j in mav1cu.plan(cfg, n)]
+    state = np.zeros(1, PLANNER_DTYPE)
+    buf = np.zeros(64, mav1cu.JOB_DTYPE)
+    got = []
+    for f in range(n + 1):
+        k = L.mav1cu_plan_frames(cfg.ctypes.data, state.ctypes.data, 1 if f < n else 0, 1 if f == n else 0,
+                                 buf.ctypes.data, len(buf))
+        assert k >= 0
+        got += [tuple(j) for j in buf[:k]]
+    assert got == whole
+    assert state[0]["in_disp"] == n and state[0]["inq_n"] == 0
