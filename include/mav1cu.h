@@ -190,6 +190,16 @@ int mav1cu_cdef_select(mav1cu_session *s, int num_cdef_presets);
 /* Loop restoration of REC (CDEF output) with DBK and LRUNITS into LROUT
  * (Backend.restore, backend.h:18-19; backend_cpu.c:179-188). */
 int mav1cu_restore(mav1cu_session *s);
+/* Loop-restoration parameter search: per restoration unit of every plane,
+ * RESTORE_NONE, a least-squares Wiener filter with its greedy +-1 tap
+ * refinement, or the best self-guided set with fitted projection weights, by
+ * 16 * SSE + lambda * bits against SRC; from REC (CDEF output) and DBK (the
+ * deblocked frame). Writes LRUNITS and lr_type of the device PARAMS record
+ * (and of the next export's parameters section). lr_test: Mav1Config.lr_test
+ * (Wiener on even units, the self-guided set of least SSE on odd ones).
+ * Replaces lr_select (lr_search.c:244-359), a host step of the reference's
+ * run_frame_core (encoder.c:636-638). */
+int mav1cu_lr_search(mav1cu_session *s, int lr_test);
 
 /* Waits for the session stream; returns the sticky error state. */
 int mav1cu_synchronize(mav1cu_session *s);
@@ -346,6 +356,11 @@ int mav1cu_stream_synchronize(mav1cu_stream *st);
  *                     transform block's adjusted, at most 32 x 32, area);
  *                     the other planes of such blocks point at the zero run
  *                     (coef_off 0)
+ *   frame parameters  the mav1cu_frame_params record of the frame; with
+ *                     MAV1CU_EXPORT_LR its lr_type is the one the loop-
+ *                     restoration search chose (mav1cu_lr_search)
+ *   LR units          (MAV1CU_EXPORT_LR) the frame's mav1cu_lr_unit records,
+ *                     all planes (what tile_writer.c's write_lr reads)
  *   reconstruction    (MAV1CU_EXPORT_REC) the shown picture as
  *                     mav1_get_recon returns it (encoder.c:877-915): the
  *                     visible width x height luma samples, then each
@@ -372,9 +387,13 @@ typedef struct {
   int64_t rec_off;
   int64_t rec_bytes;   /* bytes of the reconstruction section (0 without MAV1CU_EXPORT_REC) */
   int64_t bytes;       /* bytes the export wrote: header and sections */
+  int64_t params_off;  /* the frame's mav1cu_frame_params (lr_type as the LR search chose it) */
+  int64_t lr_off;      /* lr_units mav1cu_lr_unit records (MAV1CU_EXPORT_LR) */
+  int32_t lr_units;
+  int32_t pad;
 } mav1cu_export_header;
 
-enum { MAV1CU_EXPORT_REC = 1 };
+enum { MAV1CU_EXPORT_REC = 1, MAV1CU_EXPORT_LR = 2 };
 
 /* Bytes an export image of this session may need. */
 size_t mav1cu_export_capacity(const mav1cu_session *s);
@@ -434,14 +453,16 @@ void mav1cu_build_fwd_matrices(int32_t *mats);
  * at start-up or whose other streams must not be stalled by cudaMalloc /
  * cudaFree. `params` is a device copy of the frame's mav1cu_frame_params;
  * `blocks` / `sbs` are the analysis output (num_sbs superblocks);
- * mi_rows / mi_cols are the frame's size in 4x4 units and must match params.
+ * mi_rows / mi_cols are the frame's size in 4x4 units and must equal params'
+ * mi_rows / mi_cols: blocks at or beyond the given size are left unchanged.
  * Scratch is a fixed device array of 2 x 1,048,576 bytes per device: frames
  * above 1,048,576 4x4 units (4096 x 4096 luma samples) are refused with
  * MAV1CU_ERR_ARG. Each call clears the scratch it uses first. Calls that
  * overlap in time on one device share that scratch and race: order them on
- * one stream or with events. The first call on each device looks up the
- * scratch address (it may load the device code): make it before any stream
- * capture on that device. Returns MAV1CU_OK once the work is enqueued;
+ * one stream or with events. Every call looks up the scratch address on
+ * the current device (not cached, so a device reset does not leave a stale
+ * address); the first call on a device may load the device code: make it
+ * before any stream capture on that device. Returns MAV1CU_OK once the work is enqueued;
  * errors are written to err. */
 int mav1cu_edge_types_noalloc(const mav1cu_frame_params *params, mav1cu_block_info *blocks,
                               const mav1cu_sb_info *sbs, int mi_rows, int mi_cols, int num_sbs, void *stream,

@@ -114,7 +114,9 @@ HD int level_bsize(int l) { return l == 0 ? BLOCK_64X64 : l == 1 ? BLOCK_32X32 :
   X(__constant__, Cdef_Uv_Dir) X(__constant__, Cdef_Pri_Taps)                           \
   X(__constant__, Cdef_Sec_Taps) X(__constant__, Cdef_Directions)                       \
   X(__constant__, Sgr_Params) X(__constant__, Wiener_Taps_Min)                          \
-  X(__constant__, Wiener_Taps_Max)                                                      \
+  X(__constant__, Wiener_Taps_Max) X(__constant__, Wiener_Taps_K)                       \
+  X(__constant__, Wiener_Taps_Mid) X(__constant__, Sgrproj_Xqd_Min)                     \
+  X(__constant__, Sgrproj_Xqd_Max) X(__constant__, Sgrproj_Xqd_Mid)                     \
   X(__device__, Subpel_Filters) X(__device__, Dr_Intra_Derivative)                      \
   X(__device__, Sm_Weights_Tx_4x4) X(__device__, Sm_Weights_Tx_8x8)                     \
   X(__device__, Sm_Weights_Tx_16x16) X(__device__, Sm_Weights_Tx_32x32)                 \

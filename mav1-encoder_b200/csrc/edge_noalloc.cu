@@ -20,10 +20,17 @@
 // different host threads) share it and race; order such calls on one stream
 // or with events.
 //
-// Set-up: the first call on each device looks up the array's device address
-// with cudaGetSymbolAddress while that device is current; this may load the
-// library's device code on that device. Make that first call before any
-// stream capture on the device.
+// Set-up: every call looks up the array's device address with
+// cudaGetSymbolAddress while the caller's device is current (the address is
+// not cached: after cudaDeviceReset, or once the primary context is
+// destroyed and made again, the array may sit elsewhere). The first call on
+// a device may load the library's device code on it: make that first call
+// before any stream capture on the device.
+//
+// Sizes: mi_rows / mi_cols must equal the frame's (params->mi_rows /
+// mi_cols); the scratch is sized by them. Blocks at or beyond that size are
+// left unchanged, so a caller passing a smaller size than the frame's gets
+// those blocks' bits 4 / 5 as they were.
 //
 // The algorithm is get_filter_type( ) of the AV1 specification (7.11.2) as
 // the reference runs it on the host (src/encoder.c:319-346): mark every 4x4
@@ -34,14 +41,11 @@
 #include <stdarg.h>
 #include <stdio.h>
 
-#include <mutex>
-
 #include "common.cuh"
 
 namespace noalloc {
 
 constexpr int MAX_MI = 1024 * 1024;  // 4x4 units per map: 4096 x 4096 luma
-constexpr int MAX_DEVICES = 64;
 
 static __device__ __align__(256) uint8_t scratch[2 * MAX_MI];
 
@@ -80,9 +84,6 @@ __global__ void k_types(const FrameParams *fp, BlockInfo *blocks, const SbInfo *
   b->interp_filter = (b->interp_filter & 15) | fy << 4 | fuv << 5;
 }
 
-static std::mutex setup_mu;
-static uint8_t *scratch_ptr[MAX_DEVICES];
-
 static int fail(char *err, size_t errlen, int rc, const char *fmt, ...) {
   if (err && errlen) {
     va_list ap;
@@ -113,21 +114,12 @@ extern "C" int mav1cu_edge_types_noalloc(const mav1cu_frame_params *params, mav1
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess)
     return fail(err, errlen, MAV1CU_ERR_CUDA, "edge types (no-alloc): cudaGetDevice: %s", cudaGetErrorString(e));
-  if (dev < 0 || dev >= MAX_DEVICES)
-    return fail(err, errlen, MAV1CU_ERR_ARG, "edge types (no-alloc): device %d beyond %d", dev, MAX_DEVICES);
-  uint8_t *base;
-  {
-    std::lock_guard<std::mutex> lock(setup_mu);
-    if (!scratch_ptr[dev]) {
-      void *p = nullptr;
-      e = cudaGetSymbolAddress(&p, scratch);
-      if (e != cudaSuccess || !p)
-        return fail(err, errlen, MAV1CU_ERR_CUDA, "edge types (no-alloc): scratch address on device %d: %s", dev,
-                    cudaGetErrorString(e));
-      scratch_ptr[dev] = (uint8_t *)p;
-    }
-    base = scratch_ptr[dev];
-  }
+  void *p = nullptr;
+  e = cudaGetSymbolAddress(&p, scratch);
+  if (e != cudaSuccess || !p)
+    return fail(err, errlen, MAV1CU_ERR_CUDA, "edge types (no-alloc): scratch address on device %d: %s", dev,
+                cudaGetErrorString(e));
+  uint8_t *base = (uint8_t *)p;
   size_t cells = (size_t)mi_rows * mi_cols;
   uint8_t *ys = base, *uvs = base + cells;
   cudaStream_t st = (cudaStream_t)stream;

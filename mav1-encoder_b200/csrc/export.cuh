@@ -22,6 +22,8 @@
 // plane it replaces, which is not copied.
 #pragma once
 
+#include <stddef.h>
+
 #include "common.cuh"
 
 namespace xport {
@@ -41,8 +43,26 @@ constexpr int STORE_CTAS = MAV1CU_STORE_CTAS;
 struct Header {  // mav1cu_export_header
   int32_t status, seq, num_sbs, num_blocks, num_coefs, zero_run;
   int64_t sbs_off, cdef_off, blocks_off, coefs_off, rec_off, rec_bytes, bytes;
+  int64_t params_off, lr_off;
+  int32_t lr_units, pad;
 };
-static_assert(sizeof(Header) == 80, "export header layout");
+static_assert(sizeof(Header) == 104, "export header layout");
+
+// The frame parameters (the host's record, passed by value, with lr_type as
+// the loop-restoration search chose it) and the LR units in use, into their
+// sections. The rest of the image is written by the other export kernels.
+__global__ void k_export_side(FrameParams fp, const int *lrTypes, const LrUnit *units, uint8_t *image, Header layout) {
+  int *pdst = (int *)(image + layout.params_off);
+  const int *psrc = (const int *)&fp;
+  const int nparams = (int)(sizeof(FrameParams) / 4), lrType = (int)(offsetof(FrameParams, lr_type) / 4);
+  int t = blockIdx.x * blockDim.x + threadIdx.x, n = gridDim.x * blockDim.x;
+  for (int k = t; k < nparams; k += n)
+    pdst[k] = layout.lr_units > 0 && k >= lrType && k < lrType + 3 ? lrTypes[k - lrType] : psrc[k];
+  int *udst = (int *)(image + layout.lr_off);
+  const int *usrc = (const int *)units;
+  int nwords = layout.lr_units * (int)(sizeof(LrUnit) / 4);
+  for (int k = t; k < nwords; k += n) udst[k] = usrc[k];
+}
 
 // The frame parameters the packing depends on, passed by value: the export
 // runs on its own stream and must not read PARAMS, which the next frame's
@@ -208,7 +228,8 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_export_scan(const int4 *counts
     h.num_coefs = (int32_t)ncoefs;
     h.zero_run = zrun;
     h.bytes = fits ? (long long)sizeof(Header) + (long long)num_sbs * (SB_WORDS * 4 + 1) + nblocks * BLK_WORDS * 4 +
-                         ncoefs * 4 + layout.rec_bytes
+                         ncoefs * 4 + (long long)sizeof(FrameParams) + (long long)layout.lr_units * sizeof(LrUnit) +
+                         layout.rec_bytes
                    : (long long)sizeof(Header);
     if (!fits) h.rec_bytes = 0;
     *(Header *)image = h;

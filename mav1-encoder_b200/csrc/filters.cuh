@@ -385,9 +385,12 @@ HD int lr_src(const FrameParams *fp, int plane, const LrBlock *lb, const uint8_t
   return cdef[fp->offset[plane] + y * stride + x];
 }
 
-// Wiener filter (spec 7.17.4, 8-bit rounding).
-HD void lr_wiener(const FrameParams *fp, int plane, const LrBlock *lb, const uint8_t *cdef, const uint8_t *dbk,
-                  uint8_t *out, const LrUnit *u) {
+// Wiener filter (spec 7.17.4, 8-bit rounding). Each output sample goes to
+// sink(offset in the plane buffer, value): the apply kernel stores it, the
+// parameter search accumulates its squared error.
+template <class Sink>
+HD void lr_wiener_to(const FrameParams *fp, int plane, const LrBlock *lb, const uint8_t *cdef, const uint8_t *dbk,
+                     const LrUnit *u, Sink &sink) {
   int vf[7], hf[7];
   vf[3] = 128;
   hf[3] = 128;
@@ -412,8 +415,19 @@ HD void lr_wiener(const FrameParams *fp, int plane, const LrBlock *lb, const uin
     for (int c = 0; c < lb->w; c++) {
       int s = 0;
       for (int t = 0; t < 7; t++) s += vf[t] * inter[r + t][c];
-      out[fp->offset[plane] + (lb->y + r) * stride + lb->x + c] = (uint8_t)clip3(0, 255, round2(s, round1));
+      sink(fp->offset[plane] + (lb->y + r) * stride + lb->x + c, clip3(0, 255, round2(s, round1)));
     }
+}
+
+struct StoreSink {
+  uint8_t *out;
+  HD void operator()(int o, int v) { out[o] = (uint8_t)v; }
+};
+
+HD void lr_wiener(const FrameParams *fp, int plane, const LrBlock *lb, const uint8_t *cdef, const uint8_t *dbk,
+                  uint8_t *out, const LrUnit *u) {
+  StoreSink sink{out};
+  lr_wiener_to(fp, plane, lb, cdef, dbk, u, sink);
 }
 
 // Box filter (spec 7.17.3); F gets w x h values (row stride 4).
@@ -469,12 +483,11 @@ HD void lr_box(const FrameParams *fp, int plane, const LrBlock *lb, const uint8_
   }
 }
 
-// Self-guided filter (spec 7.17.2).
-HD void lr_sgr(const FrameParams *fp, int plane, const LrBlock *lb, const uint8_t *cdef, const uint8_t *dbk, uint8_t *out,
-               const LrUnit *u) {
-  int flt0[16], flt1[16];
-  lr_box(fp, plane, lb, cdef, dbk, u->set, 0, flt0);
-  lr_box(fp, plane, lb, cdef, dbk, u->set, 1, flt1);
+// Self-guided projection (spec 7.17.2) of a block whose box-filter outputs
+// are flt0 / flt1, into sink(offset, value).
+template <class Sink>
+HD void lr_sgr_project(const FrameParams *fp, int plane, const LrBlock *lb, const uint8_t *cdef, const LrUnit *u,
+                       const int *flt0, const int *flt1, Sink &sink) {
   int w0 = u->xqd[0], w1 = u->xqd[1];
   int w2 = (1 << SGRPROJ_PRJ_BITS) - w0 - w1;
   int r0 = T(Sgr_Params)[u->set][0], r1 = T(Sgr_Params)[u->set][2];
@@ -486,8 +499,18 @@ HD void lr_sgr(const FrameParams *fp, int plane, const LrBlock *lb, const uint8_
       int v = w1 * uu;
       v += r0 ? w0 * flt0[i * 4 + j] : w0 * uu;
       v += r1 ? w2 * flt1[i * 4 + j] : w2 * uu;
-      out[o] = (uint8_t)clip3(0, 255, round2(v, SGRPROJ_RST_BITS + SGRPROJ_PRJ_BITS));
+      sink(o, clip3(0, 255, round2(v, SGRPROJ_RST_BITS + SGRPROJ_PRJ_BITS)));
     }
+}
+
+// Self-guided filter (spec 7.17.2).
+HD void lr_sgr(const FrameParams *fp, int plane, const LrBlock *lb, const uint8_t *cdef, const uint8_t *dbk, uint8_t *out,
+               const LrUnit *u) {
+  int flt0[16], flt1[16];
+  lr_box(fp, plane, lb, cdef, dbk, u->set, 0, flt0);
+  lr_box(fp, plane, lb, cdef, dbk, u->set, 1, flt1);
+  StoreSink sink{out};
+  lr_sgr_project(fp, plane, lb, cdef, u, flt0, flt1, sink);
 }
 
 // Thread per (plane, 4x4 luma block): loop_restore_block( ) with the unit's

@@ -23,6 +23,7 @@
 #include "filters.cuh"
 #include "stream.cuh"
 #include "export.cuh"
+#include "lrsearch.cuh"
 
 // dynamic shared memory of the analysis pass-1 kernel for candidate groups of
 // `group` threads: a WarpMem (edge scratch) per group (per warp for CTA groups)
@@ -93,6 +94,9 @@ struct mav1cu_session {
   cudaEvent_t xring[XRING];  // completion of export seq, recorded at xring[seq % XRING] (blocking sync)
   int device;              // the device the session's memory lives on
   cudaStream_t ss;         // status reads of host consumers (never waits for the session's other streams)
+  lrs::Fit *lrfit;         // loop-restoration search: first-pass results per restoration unit
+  int *lr_types;           // the search's lr_type per plane (exported with the frame)
+  int max_lr_units;
   std::vector<int> wave_start, wave_len;
   int wave_tile_w;
   FrameParams fp;          // host copy of the current parameters
@@ -261,7 +265,7 @@ static void free_all(mav1cu_session *s) {
     if (s->buf[i]) cudaFree(s->buf[i]);
   void *extra[] = {s->qp[0], s->qp[1], s->dsrc, s->dref[0], s->dref[1], s->ys, s->uvs, s->waves, s->status, s->blk_at, s->blk_list,
                    s->blk_done, s->mats_t, s->dep_count, s->succ_count, s->succ, s->queue, s->corners,
-                   s->xcounts, s->xblk_base, s->xcoef_base, s->xmeta};
+                   s->xcounts, s->xblk_base, s->xcoef_base, s->xmeta, s->lrfit, s->lr_types};
   for (void *p : extra)
     if (p) cudaFree(p);
   if (s->ximage) cudaFreeHost(s->ximage);
@@ -330,6 +334,10 @@ extern "C" int mav1cu_session_create(int width, int height, int max_cdef_presets
   if (e == cudaSuccess) e = cudaMalloc(&s->xblk_base, sizeof(int) * nsb);
   if (e == cudaSuccess) e = cudaMalloc(&s->xcoef_base, sizeof(int) * nsb);
   if (e == cudaSuccess) e = cudaMalloc(&s->xmeta, sizeof(int) * 4);
+  s->max_lr_units = 3 * (g.sb_rows + 1) * (g.sb_cols + 1);
+  if (e == cudaSuccess) e = cudaMalloc(&s->lrfit, sizeof(lrs::Fit) * s->max_lr_units);
+  if (e == cudaSuccess) e = cudaMalloc(&s->lr_types, sizeof(int) * 4);
+  if (e == cudaSuccess) e = cudaMemset(s->lr_types, 0, sizeof(int) * 4);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->own_stream, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->xs, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->x_fork, cudaEventDisableTiming);
@@ -673,6 +681,24 @@ extern "C" int mav1cu_restore(mav1cu_session *s) {
   return after_launch(s, "loop restoration");
 }
 
+// Units of every plane of the current frame (the LRUNITS records in use).
+static int lr_units_of(const FrameParams &fp) { return fp.lr_unit_off[2] + fp.lr_unit_rows[2] * fp.lr_unit_cols[2]; }
+
+extern "C" int mav1cu_lr_search(mav1cu_session *s, int lr_test) {
+  if (need_params(s)) return s->err;
+  int n = lr_units_of(s->fp);
+  if (n <= 0 || n > s->max_lr_units) return set_error(s, MAV1CU_ERR_ARG, "loop-restoration search: %d units", n);
+  export_fence(s);  // LRUNITS and the plane types are exported
+  lrs::k_lr_fit<<<n, lrs::THREADS, sizeof(lrs::Shared), s->stream>>>(DP(s), U8(s, MAV1CU_BUF_REC),
+                                                                       U8(s, MAV1CU_BUF_DBK), U8(s, MAV1CU_BUF_SRC),
+                                                                       s->lrfit);
+  if (after_launch(s, "loop-restoration fit")) return s->err;
+  lrs::k_lr_select<<<3, lrs::THREADS, sizeof(lrs::Shared), s->stream>>>(
+      (FrameParams *)s->buf[MAV1CU_BUF_PARAMS], U8(s, MAV1CU_BUF_REC), U8(s, MAV1CU_BUF_DBK), U8(s, MAV1CU_BUF_SRC),
+      s->lrfit, (LrUnit *)s->buf[MAV1CU_BUF_LRUNITS], lr_test, s->lr_types);
+  return after_launch(s, "loop-restoration selection");
+}
+
 // ---- compact export of the writer inputs ------------------------------------------
 
 static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
@@ -686,7 +712,9 @@ static xport::Header export_layout(const mav1cu_session *s) {
   h.cdef_off = (int64_t)align256(h.sbs_off + nsb * sizeof(SbInfo));
   h.blocks_off = (int64_t)align256(h.cdef_off + nsb);
   h.coefs_off = (int64_t)align256(h.blocks_off + nsb * MAX_BLOCKS_PER_SB * sizeof(BlockInfo));
-  h.rec_off = (int64_t)align256(h.coefs_off + sizeof(int32_t) * COEFS_PER_SB * nsb);
+  h.params_off = (int64_t)align256(h.coefs_off + sizeof(int32_t) * COEFS_PER_SB * nsb);
+  h.lr_off = (int64_t)align256(h.params_off + sizeof(FrameParams));
+  h.rec_off = (int64_t)align256(h.lr_off + sizeof(LrUnit) * (size_t)s->max_lr_units);
   return h;
 }
 
@@ -711,7 +739,8 @@ extern "C" void *mav1cu_export_image(mav1cu_session *s) {
 
 extern "C" int mav1cu_export(mav1cu_session *s, void *image, size_t cap, int flags) {
   if (need_params(s)) return s->err;
-  if (flags & ~MAV1CU_EXPORT_REC) return set_error(s, MAV1CU_ERR_ARG, "export: unknown flags 0x%x", flags);
+  if (flags & ~(MAV1CU_EXPORT_REC | MAV1CU_EXPORT_LR))
+    return set_error(s, MAV1CU_ERR_ARG, "export: unknown flags 0x%x", flags);
   size_t need = mav1cu_export_capacity(s);
   if (!image || cap < need || ((uintptr_t)image & 15))
     return set_error(s, MAV1CU_ERR_ARG, "export: image %p of %zu bytes (needs %zu bytes, 16-byte aligned)", image, cap,
@@ -730,6 +759,9 @@ extern "C" int mav1cu_export(mav1cu_session *s, void *image, size_t cap, int fla
   layout.seq = ++s->xseq;
   int withRec = flags & MAV1CU_EXPORT_REC;
   layout.rec_bytes = withRec ? (int64_t)i420_bytes(s->g) : 0;
+  layout.lr_units = (flags & MAV1CU_EXPORT_LR) ? lr_units_of(s->fp) : 0;
+  if (layout.lr_units < 0 || layout.lr_units > s->max_lr_units)
+    return set_error(s, MAV1CU_ERR_ARG, "export: %d loop-restoration units", layout.lr_units);
   size_t nsb = (size_t)s->g.num_sbs;
   const BlockInfo *blocks = (const BlockInfo *)s->buf[MAV1CU_BUF_BLOCKS];
   const SbInfo *sbs = (const SbInfo *)s->buf[MAV1CU_BUF_SBS];
@@ -748,6 +780,9 @@ extern "C" int mav1cu_export(mav1cu_session *s, void *image, size_t cap, int fla
       f, blocks, sbs, (int)nsb, (const int32_t *)s->buf[MAV1CU_BUF_COEFS], s->xblk_base, s->xcoef_base, s->xmeta,
       dimg, layout);
   if (after_launch(s, "export write")) return s->err;
+  xport::k_export_side<<<1, 128, 0, s->xs>>>(s->fp, s->lr_types, (const LrUnit *)s->buf[MAV1CU_BUF_LRUNITS], dimg,
+                                             layout);
+  if (after_launch(s, "export parameters")) return s->err;
   if (withRec) {
     const Geometry &g = s->g;
     int rows = g.h + 2 * ((g.h + 1) >> 1);
@@ -924,12 +959,6 @@ struct mav1cu_stream {
 extern "C" int mav1cu_stream_create(const mav1cu_config *cfg, mav1cu_stream **out, char *err, size_t errlen) {
   *out = NULL;
   drv::Norm n = drv::normalise(cfg);
-  if (n.c.restoration && n.c.qindex > 0) {
-    // run_frame_core's loop-restoration parameter search (lr_select) is a
-    // host step of the encoder; the device stream codes frames without it
-    snprintf(err, errlen, "the device stream does not run the loop-restoration search (restoration must be 0)");
-    return MAV1CU_ERR_ARG;
-  }
   mav1cu_stream *st = new mav1cu_stream();
   st->n = n;
   for (int e = 0; e < NUM_ENGINES; e++) {
@@ -1089,7 +1118,15 @@ extern "C" int mav1cu_stream_encode(mav1cu_stream *st, const mav1cu_frame_job *j
   int lfOn = fp.lf_level[0] || fp.lf_level[1] || fp.lf_level[2] || fp.lf_level[3];
   int filt = lfOn || (nPresets && !cdefOff) || !c.turbo;
   if (filt && (mav1cu_filter_info(s) || mav1cu_filter(s, presets))) return s->err;
+  // loop restoration (encoder.c:633-643): the deblocked frame is kept before
+  // CDEF selection, the search runs on the CDEF output, the restored frame
+  // replaces REC
+  int useLr = c.restoration && c.qindex > 0 && !(job->leafopt & 8);
+  if (useLr && mav1cu_copy(s, MAV1CU_BUF_DBK, MAV1CU_BUF_REC, fb)) return s->err;
   if (c.cdef && c.qindex > 0 && !cdefOff && mav1cu_cdef_select(s, nPresets)) return s->err;
+  if (useLr && (mav1cu_lr_search(s, c.lr_test) || mav1cu_copy(s, MAV1CU_BUF_LROUT, MAV1CU_BUF_REC, fb) ||
+                mav1cu_restore(s) || mav1cu_copy(s, MAV1CU_BUF_REC, MAV1CU_BUF_LROUT, fb)))
+    return s->err;
   EventRef out;
   for (int k = 0; k < 8; k++) {
     if (!((rf >> k) & 1) || !slot_exists(st->n, k)) continue;

@@ -109,7 +109,11 @@ class Encoder:
         if i420 is None:
             rc = self.lib.mav1_send_frame(self.h_, None, None)
         else:
+            if isinstance(i420, (bytes, bytearray, memoryview)):
+                i420 = np.frombuffer(i420, np.uint8)
             a = np.ascontiguousarray(i420, np.uint8).reshape(-1)
+            if a.size != self.w * self.h + 2 * self.cw * self.ch:
+                raise Mav1Error(f"frame of {a.size} bytes, expected {self.w * self.h + 2 * self.cw * self.ch}")
             y = self.w * self.h
             c = self.cw * self.ch
             base = a.ctypes.data
@@ -182,6 +186,32 @@ def encode(frames, cfg, recon=True, counters=None):
             counters.append(enc.counters())
     finally:
         enc.close()
+    return packets, recons
+
+
+def code_frames(enc, frames, expect, recon=True, timeout_ms=60000):
+    """Sends frames to a live encoder (no flush) and receives `expect`
+    temporal units: the ones ready after each send, then the rest as they
+    complete. With closed GOPs (the frames start at a key frame and end at
+    the next key-frame boundary), every frame's temporal unit comes out
+    without a flush, so one encoder can code clip after clip. Returns
+    (packets, reconstructions)."""
+    packets, recons = [], []
+
+    def drain(wait):
+        while len(packets) < expect:
+            r = enc.receive(recon, wait_ms=timeout_ms if wait else None)
+            if r is None:
+                if wait:
+                    raise Mav1Error(f"no temporal unit within {timeout_ms} ms ({len(packets)} of {expect})")
+                return
+            packets.append(r[0])
+            recons.append(r[1])
+
+    for f in frames:
+        enc.send(f)
+        drain(False)
+    drain(True)
     return packets, recons
 
 

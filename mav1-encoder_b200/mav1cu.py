@@ -56,9 +56,11 @@ assert PARAMS_DTYPE.itemsize == 392 and BLOCK_DTYPE.itemsize == 108
 EXPORT_HEADER_DTYPE = np.dtype([
     ("status", "<i4"), ("seq", "<i4"), ("num_sbs", "<i4"), ("num_blocks", "<i4"), ("num_coefs", "<i4"),
     ("zero_run", "<i4"), ("sbs_off", "<i8"), ("cdef_off", "<i8"), ("blocks_off", "<i8"), ("coefs_off", "<i8"),
-    ("rec_off", "<i8"), ("rec_bytes", "<i8"), ("bytes", "<i8")])
+    ("rec_off", "<i8"), ("rec_bytes", "<i8"), ("bytes", "<i8"), ("params_off", "<i8"), ("lr_off", "<i8"),
+    ("lr_units", "<i4"), ("pad", "<i4")])
 EXPORT_REC = 1
-assert SB_DTYPE.itemsize == 356 and LRUNIT_DTYPE.itemsize == 48 and EXPORT_HEADER_DTYPE.itemsize == 80
+EXPORT_LR = 2
+assert SB_DTYPE.itemsize == 356 and LRUNIT_DTYPE.itemsize == 48 and EXPORT_HEADER_DTYPE.itemsize == 104
 
 EXPORTS = [
     "mav1cu_session_create", "mav1cu_session_destroy", "mav1cu_set_stream", "mav1cu_get_stream", "mav1cu_buf_size",
@@ -69,7 +71,9 @@ EXPORTS = [
     "mav1cu_frame_params_for", "mav1cu_stream_create", "mav1cu_stream_destroy", "mav1cu_stream_session",
     "mav1cu_stream_encode", "mav1cu_stream_slot", "mav1cu_stream_engines", "mav1cu_stream_engine",
     "mav1cu_stream_wait", "mav1cu_stream_join", "mav1cu_stream_synchronize", "mav1cu_edge_types_noalloc",
-    "mav1cu_export_capacity", "mav1cu_export_image", "mav1cu_export",
+    "mav1cu_export_capacity", "mav1cu_export_image", "mav1cu_export", "mav1cu_lr_search", "mav1cu_plan_frames",
+    "mav1cu_layout_of", "mav1cu_export_seq", "mav1cu_export_wait", "mav1cu_export_query", "mav1cu_host_alloc",
+    "mav1cu_host_free",
 ]
 
 
@@ -100,6 +104,8 @@ def load_library(path=LIB_PATH):
         getattr(lib, f).argtypes = [vp]
         getattr(lib, f).restype = i32
     lib.mav1cu_filter.argtypes = [vp, i32]
+    lib.mav1cu_lr_search.argtypes = [vp, i32]
+    lib.mav1cu_lr_search.restype = i32
     lib.mav1cu_cdef_select.argtypes = [vp, i32]
     lib.mav1cu_error_string.argtypes = [vp]
     lib.mav1cu_error_string.restype = ctypes.c_char_p
@@ -257,6 +263,9 @@ class Session:
 
     def restore(self):
         self._check(self.lib.mav1cu_restore(self.h), "restore")
+
+    def lr_search(self, lr_test=0):
+        self._check(self.lib.mav1cu_lr_search(self.h, lr_test), "lr_search")
 
     def synchronize(self):
         self._check(self.lib.mav1cu_synchronize(self.h), "synchronize")

@@ -7,7 +7,7 @@ import numpy as np
 import mav1cu
 import oracle
 import synthetic
-from mav1cu import BLOCK_DTYPE, PARAMS_DTYPE, SB_DTYPE
+from mav1cu import BLOCK_DTYPE, LRUNIT_DTYPE, PARAMS_DTYPE, SB_DTYPE
 
 ST = oracle.STAGE
 NUM_NODES, A_SLOTS = 85, 13
@@ -187,10 +187,29 @@ class FrameCheck:
         self.s.restore()
         return {"lrout": diff(self.s.download("LROUT", count=self.fb), self.snap("RESTORE", "LROUT", self.fb))}
 
+    def lr_search(self):
+        """The loop-restoration search (lr_select, lr_search.c:244-359) on the
+        oracle's CDEF output and deblocked frame: every unit record in use and
+        each plane's lr_type."""
+        if (ST["LRSEL"], "LRUNITS") not in self.fr:
+            return {}
+        self.frame_inputs()
+        self.s.upload("REC", self.snap("CDEFSEL", "REC", self.fb))
+        self.s.upload("DBK", self.snap("LRSEL", "DBK", self.fb))
+        self.s.lr_search(int(self.cfg.lr_test))
+        p = self.p
+        n = int(p["lr_unit_off"][2] + p["lr_unit_rows"][2] * p["lr_unit_cols"][2])
+        got = self.s.download("LRUNITS", LRUNIT_DTYPE, count=n)
+        want = self.snap("LRSEL", "LRUNITS", n * LRUNIT_DTYPE.itemsize).view(LRUNIT_DTYPE)
+        gp = self.s.download("PARAMS", np.uint8, count=392).view(PARAMS_DTYPE)[0]
+        wp = self.fr[(ST["LRSEL"], "PARAMS")][:392].copy().view(PARAMS_DTYPE)[0]
+        bad = [i for i in range(n) if got[i].tobytes() != want[i].tobytes()]
+        return {"lrunits": len(bad), "lr_type": int((gp["lr_type"] != wp["lr_type"]).sum())}
+
     def chain(self):
         """Every stage on the device from the frame inputs only, in
-        run_frame_core's order (encoder.c:599-657); loop-restoration
-        parameters come from the host search (lr_select) as in the encoder."""
+        run_frame_core's order (encoder.c:599-657), the loop-restoration
+        search included."""
         self.frame_inputs()
         self.s.upload("REC", self.snap("PARAMS", "REC", self.fb))
         self.s.upload("COEFS", self.snap("PARAMS", "COEFS", self.s.size("COEFS")))
@@ -206,8 +225,7 @@ class FrameCheck:
             self.s.cdef_select(self.state["num_cdef_presets"])
         final = "REC"
         if use_lr:
-            self.s.set_params(self.fr[(ST["LRSEL"], "PARAMS")][:392].copy())
-            self.s.upload("LRUNITS", self.snap("LRSEL", "LRUNITS", self.s.size("LRUNITS")))
+            self.s.lr_search(int(self.cfg.lr_test))
             self.s.copy("LROUT", "REC")
             self.s.restore()
             final = "LROUT"
@@ -242,7 +260,7 @@ def first_block_mismatch(a, b, skip=()):
     return None
 
 
-STAGES = ("me", "analyze", "edge", "recon", "finfo", "filter", "cdef_select", "restore", "chain")
+STAGES = ("me", "analyze", "edge", "recon", "finfo", "filter", "cdef_select", "lr_search", "restore", "chain")
 
 
 def check_all(sess, tr, cfg, stages=STAGES):
@@ -439,6 +457,7 @@ def export_vs_packed(image, blocks, sbs, coefs, cdef, p):
     out["blocks"] = int((iblocks != want["blocks"]).sum()) if len(iblocks) == len(want["blocks"]) else -1
     out["levels"] = int((ilevels != want["levels"]).sum()) if len(ilevels) == len(want["levels"]) else -1
     nbytes = (mav1cu.EXPORT_HEADER_DTYPE.itemsize + len(isbs) * SB_DTYPE.itemsize + len(icdef) +
-              len(iblocks) * BLOCK_DTYPE.itemsize + 4 * len(ilevels) + (0 if irec is None else len(irec)))
+              len(iblocks) * BLOCK_DTYPE.itemsize + 4 * len(ilevels) + mav1cu.PARAMS_DTYPE.itemsize +
+              mav1cu.LRUNIT_DTYPE.itemsize * int(h["lr_units"]) + (0 if irec is None else len(irec)))
     out["bytes"] = int(h["bytes"] != nbytes)
     return out

@@ -84,9 +84,6 @@ def test_bad_arguments_rejected_without_device_work():
     assert lib.mav1cu_session_create(8, 8, 4, ctypes.byref(h), err, 256) == -1
     assert b"unsupported" in err.value
     assert lib.mav1cu_session_create(64, 64, 5, ctypes.byref(h), err, 256) == -1
-    cfg = mav1cu.cli_config(64, 64, q=100, lr=1)
-    assert lib.mav1cu_stream_create(cfg.ctypes.data, ctypes.byref(h), err, 256) == -1
-    assert b"loop-restoration" in err.value
     jobs = np.zeros(2, mav1cu.JOB_DTYPE)
     assert lib.mav1cu_plan(mav1cu.cli_config(64, 64, turbo=1).ctypes.data, 10, jobs.ctypes.data, 2) == -1
 

@@ -91,3 +91,14 @@ def test_noalloc_matches_session_entry_point_two_calls_in_a_row():
     for c, d in zip(cases, dev):
         got = d["blocks"].cpu().numpy()
         assert np.array_equal(got, c["after"])
+
+    # the calls allocate nothing: after the warm-up above, further calls on
+    # the same stream leave the device's free memory as it was
+    free0, _ = torch.cuda.mem_get_info()
+    for _ in range(3):
+        for c, d in zip(cases, dev):
+            rc, msg = call(lib, d["params"], d["blocks"], d["sbs"], c["geom"], stream.cuda_stream)
+            assert rc == 0, msg
+    stream.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0
