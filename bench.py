@@ -33,6 +33,7 @@ Multi-GPU: the path does not shard (one stream is a serial reference
 chain); --gpus N runs N independent replicas, one per GPU.
 """
 import argparse
+import hashlib
 import json
 import os
 import statistics
@@ -122,6 +123,92 @@ def split_gops(jobs):
             gops.append([])
         gops[-1].append(j)
     return gops
+
+
+def batch_bench(args):
+    """The batching workload (16 streams: 4 each of 640x360, 1280x720,
+    1920x1080, 2560x1440; 60 frames each, --turbo, q from {80, 125, 170}):
+    every stream through its own live encoder, all at once, against the same
+    streams coded one after another. Each stream's IVF is checked against the
+    oracle's hashes (tests/golden/batch_hashes.json). Wall clock, sources from
+    host memory, entropy coding included."""
+    import batch
+    import mav1cu
+
+    specs = synthetic.batch_streams()
+    frames = batch.load_streams([s for s, _ in specs])
+    # keyint = clip length: the clip codes as with keyint 0 (one key frame),
+    # and a live encoder codes it again as a new closed GOP at every pass
+    cfgs = [mav1cu.cli_config(s.width, s.height, q=q, turbo=1, keyint=s.frames) for s, q in specs]
+    os.environ.setdefault("MAV1_CUDA_IMAGES", "3")
+    B = batch.Batch(list(zip(cfgs, frames)))
+    try:
+        want = {}
+        path = os.path.join(ROOT, "tests", "golden", "batch_hashes.json")
+        if os.path.exists(path):
+            want = json.load(open(path))
+        _, out = B.code(concurrent=True)
+        bitexact = None
+        if want:
+            bitexact = all(batch.stream_hashes(o, s.width, s.height) == want[s.name]["ivf"]
+                           for (s, _), o in zip(specs, out))
+        n = max(1, args.batch_passes)
+        seq = [B.code(concurrent=False)[0] for _ in range(n)]
+        conc = [B.code(concurrent=True)[0] for _ in range(n)]
+    finally:
+        B.close()
+    nframes = sum(s.frames for s, _ in specs)
+    npx = sum(s.frames * s.width * s.height for s, _ in specs)
+    fps_seq, fps_conc = nframes / (sum(seq) / n), nframes / (sum(conc) / n)
+    return {"workload": "16 streams (4 x 640x360, 4 x 1280x720, 4 x 1920x1080, 4 x 2560x1440), 60 frames each, "
+                        "--turbo, q in {80, 125, 170}; host frames in, IVF out",
+            "frames": nframes, "fps_concurrent": round(fps_conc, 1), "fps_sequential": round(fps_seq, 1),
+            "speedup": round(fps_conc / fps_seq, 3), "passes": n,
+            "mpx_per_s_concurrent": round(npx / (sum(conc) / n) / 1e6, 1),
+            "bitexact_to_oracle": bitexact}
+
+
+def serving_bench(args, capacity_pxs):
+    """The serving workload: an open-loop Poisson arrival of sessions
+    (resolution mix 640x360 0.3, 1280x720 0.4, 1920x1080 0.25, 3840x2160
+    0.05; 30-300 frames; q 60-200; --turbo), frames arriving in real time at
+    30 per second, admitted against a 150 GB device-memory budget. The arrival
+    rate offers 80% of the batched capacity (capacity_pxs: pixels per second
+    of the batching workload, all streams at once). Reports per-frame latency
+    percentiles and the aggregate rate; a sample of the sessions is coded
+    again alone and must give the same bitstream as in the mix."""
+    import batch
+    import mav1api
+    import serve
+
+    specs = serve.content_specs()
+    flat = [c for v in specs.values() for c in v]
+    clips = dict(zip([c.name for c in flat], batch.load_streams(flat)))
+    mean_len = 165.0
+    px_per_frame = serve.mean_pixels_per_second() / serve.FPS
+    rate = 0.8 * capacity_pxs / (px_per_frame * mean_len)
+    sessions = serve.poisson_sessions(args.serving_sessions, rate, seed=11)
+    for s in sessions:
+        cands = specs[(s.width, s.height)]
+        s.clip = clips[cands[s.sid % len(cands)].name]
+    os.environ.setdefault("MAV1_CUDA_IMAGES", "2")
+    srv = serve.Server(budget_bytes=150e9)
+    try:
+        wall = srv.run(sessions)
+    finally:
+        srv.close()
+    res = serve.summary(sessions, wall)
+    # alone == in the mix: re-code a sample of the sessions, each alone
+    sample = [s for s in sessions if s.latencies][:: max(1, len(sessions) // 8)][:8]
+    same = []
+    for s in sample:
+        pk, _ = mav1api.encode([s.frame(i) for i in range(s.frames)], s.config(), recon=False)
+        same.append(hashlib.sha256(mav1api.ivf_bytes(pk, s.width, s.height)).hexdigest() == s.ivf_sha256)
+    res.update({"arrival_rate_per_s": round(rate, 3), "offered_load": 0.8, "capacity_mpx_s": round(capacity_pxs / 1e6, 1),
+                "hbm_budget_gb": 150, "peak_active_sessions": srv.peak_active,
+                "peak_device_gb": round(srv.peak_bytes / 1e9, 2), "encoders_created": srv.encoders_created,
+                "alone_equals_mix": f"{sum(same)}/{len(same)}"})
+    return res
 
 
 def max_over_ranks(values, device):
@@ -427,11 +514,26 @@ def main():
     ap.add_argument("--cpu-sample", type=int, default=REF_SAMPLE, help="frames of the CPU baseline sample")
     ap.add_argument("--no-roofline", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batch", action="store_true", help="skip the 16-stream batching measurement")
+    ap.add_argument("--batch-passes", type=int, default=2)
+    ap.add_argument("--workload", default="clip", choices=["clip", "serving"],
+                    help="serving: the session-serving measurement alone (about two minutes)")
+    ap.add_argument("--serving-sessions", type=int, default=400)
     ap.add_argument("--profile-frames", type=int, default=0,
                     help="code the clip's first N planned frames once and exit (a short run for ncu)")
     args = ap.parse_args()
     if args.profile_frames:
         profile_run(args.profile_frames)
+        return
+    if args.workload == "serving":
+        import torch
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+        b = batch_bench(args)
+        with Clocks(int(os.environ.get("LOCAL_RANK", 0))) as clk:
+            res = serving_bench(args, b["mpx_per_s_concurrent"] * 1e6)
+        res["clocks"] = clk.summary()
+        res["batch"] = b
+        print(json.dumps({"workload": "serving", **res}))
         return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -491,6 +593,8 @@ def main():
                              "fps_one_stream": round(frames / (r["ms_seq"] * 1e-3), 2)},
                 "gpu_launches": int(r["launches"]), "clocks": r["clocks"],
                 "roofline": roofline(r["kern"], peaks)}
+        if not args.no_batch:
+            line["batch"] = batch_bench(args)
         if not args.no_cpu_baseline:
             fps, wall, ideal = cpu_reference(args.cpu_sample)
             line["cpu_baseline"] = {"value": round(fps, 3), "unit": "fps", "cores": cores, "kind": "reference",

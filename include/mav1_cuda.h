@@ -39,6 +39,22 @@ typedef struct {
 
 void mav1_cuda_get_counters(const Mav1Encoder *e, mav1_cuda_counters *out);
 
+/* Device memory an encoder holds (its frame engines, reference slots and
+ * staging: requested bytes), and what mav1_create would allocate for a
+ * configuration; -1 for an unsupported one. For admission of encoders
+ * against a device-memory budget. */
+int64_t mav1_cuda_device_bytes(const Mav1Encoder *e);
+int64_t mav1_cuda_device_bytes_for(const Mav1Config *cfg);
+
+/* Starts a new clip on an existing encoder, keeping its device memory and
+ * host buffers: waits until every frame sent so far is coded, drops packets
+ * not yet received, and takes cfg (same width and height; the rest may
+ * change). The next frame sent starts the new clip with a key frame; the
+ * bitstream equals a fresh encoder's. For servers that reuse encoders across
+ * sessions (creating and destroying device memory synchronises the GPU for
+ * every other encoder). Returns 0, or -1 for another frame size. */
+int mav1_cuda_restart(Mav1Encoder *e, const Mav1Config *cfg);
+
 #ifdef __cplusplus
 }
 #endif

@@ -201,6 +201,15 @@ int mav1cu_restore(mav1cu_session *s);
  * run_frame_core (encoder.c:636-638). */
 int mav1cu_lr_search(mav1cu_session *s, int lr_test);
 
+/* Failure detection without a device fault (a test hook): the session's next
+ * mav1cu_recon counts one more luma dependency for intra block hold_block
+ * than exists, so that block is never released, and its dependency waits
+ * give up after spin_limit polls instead of about 2^22. The waiting workers
+ * then set the session's device status and stop; the launch returns, the
+ * context stays usable, and mav1cu_synchronize reports MAV1CU_ERR_DEVICE.
+ * The session stays in error afterwards. No counterpart in the reference. */
+int mav1cu_debug_recon_fault(mav1cu_session *s, int hold_block, int spin_limit);
+
 /* Waits for the session stream; returns the sticky error state. */
 int mav1cu_synchronize(mav1cu_session *s);
 /* Message of the first error (empty string if none). */
@@ -338,6 +347,17 @@ int mav1cu_stream_wait(mav1cu_stream *st, void *stream);
 int mav1cu_stream_join(mav1cu_stream *st, void *stream);
 /* Waits for every engine; returns the first sticky error. */
 int mav1cu_stream_synchronize(mav1cu_stream *st);
+/* Starts a new clip on an existing stream (its device memory reused): waits
+ * for its work, takes cfg (same width and height; the other settings may
+ * change) and forgets the slot history. The next frame must be a key frame.
+ * No counterpart in the reference, whose encoders code one clip each. */
+int mav1cu_stream_reconfigure(mav1cu_stream *st, const mav1cu_config *cfg);
+/* Device memory of a stream: what its engines and slots allocated (requested
+ * bytes), and the same figure for a configuration before creating it (for
+ * admission against a memory budget). */
+int64_t mav1cu_stream_device_bytes(const mav1cu_stream *st);
+int64_t mav1cu_stream_bytes_for(const mav1cu_config *cfg);
+int64_t mav1cu_session_device_bytes(const mav1cu_session *s);
 
 /* ---- compact export of the writer inputs ---------------------------------
  * No counterpart in the reference: its Metal backend shares full-size

@@ -263,7 +263,6 @@ __device__ void wiener_fit(const FrameParams *fp, const Geom &g, const uint8_t *
                            const uint8_t *src, Shared &sh, int out[2][3]) {
   const int plane = g.plane, first = plane ? 1 : 0, nc = 3 - first, nacc = nc * nc + nc;
   const int sub = plane > 0, bwf = MI_SIZE >> sub;
-  const int ncols = g.c1 - g.c0;
   const int stride = fp->stride[plane];
   if (threadIdx.x < 7) {
     sh.f[threadIdx.x] = threadIdx.x == 3 ? 1.0 : 0.0;

@@ -77,6 +77,13 @@ struct Ctx {
   // per intra block, BlockDecoded of its corner units: bit 0 / 1 luma
   // above-right / below-left, bit 2 / 3 the same for chroma
   int *corners;
+  // polls a dependency wait makes before it gives up (sets the error and
+  // abort words); SPIN_LIMIT unless a test shortens it
+  int spin_limit;
+  // a block index whose luma dependencies are counted once more than they
+  // are, so it is never released (-1: none): the failure-detection test's
+  // never-released dependency
+  int hold;
 };
 
 #define MAX_SUCC 96  // successors per block: at most 25 along each edge, with margin
@@ -755,7 +762,7 @@ __device__ int decoded(const Ctx &c, const Smem &sm, int plane, int y, int x, in
   return y < top || x < left;
 }
 
-#define SPIN_LIMIT (1 << 22)  // polls of at least one L2 round trip each: about a second
+#define SPIN_LIMIT (1 << 22)  // polls of at least one L2 round trip each: about a second (Ctx::spin_limit)
 
 // Block index covering 4x4 luma unit (r, col) (the frame's map, built
 // before the launch).
@@ -784,7 +791,7 @@ __device__ void wait_units(const Ctx &c, const Smem &sm, int group, const int *r
     if (b == sm.me || (unsigned)b >= (unsigned)nblk) continue;
     int spins = 0;
     while (!vdone[b]) {
-      if (vstatus[1] || ++spins > SPIN_LIMIT) {
+      if (vstatus[1] || ++spins > c.spin_limit) {
         if (!vstatus[1]) {
           atomicExch(c.status, 1);
           atomicExch(c.status + 1, 1);
@@ -1395,6 +1402,7 @@ __global__ void __launch_bounds__(128) k_block_deps(Ctx c, const int *list, cons
       }
     }
     for (int off = 16; off > 0; off >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, off);
+    cnt += me == c.hold;
     if (lane == 0) {
       if (cnt == 0) push_ready(c, me);
       else c.dep_count[me] = cnt;
@@ -1440,7 +1448,7 @@ __global__ void __launch_bounds__(INTRA_THREADS, 1) k_recon_blocks(Ctx cg, Claim
         volatile int *vslot = c.queue + slot;
         int spins = 0;
         while (!*vslot && !vstatus[1]) {
-          if (++spins > SPIN_LIMIT) {
+          if (++spins > c.spin_limit) {
             atomicExch(c.status, 1);
             atomicExch(c.status + 1, 1);
             break;

@@ -97,6 +97,9 @@ struct mav1cu_session {
   lrs::Fit *lrfit;         // loop-restoration search: first-pass results per restoration unit
   int *lr_types;           // the search's lr_type per plane (exported with the frame)
   int max_lr_units;
+  int lr_searched;         // the current frame's LR units and types come from mav1cu_lr_search
+  int64_t device_bytes;    // device memory this session allocated
+  int fault_hold, fault_spins;  // failure-detection test: the next recon's held block and poll limit
   std::vector<int> wave_start, wave_len;
   int wave_tile_w;
   FrameParams fp;          // host copy of the current parameters
@@ -278,6 +281,39 @@ static void free_all(mav1cu_session *s) {
   if (s->own_stream) cudaStreamDestroy(s->own_stream);
 }
 
+// Device allocation counted into the session's footprint.
+static cudaError_t dmalloc(mav1cu_session *s, void **p, size_t bytes) {
+  cudaError_t e = cudaMalloc(p, bytes);
+  if (e == cudaSuccess) s->device_bytes += (int64_t)bytes;
+  return e;
+}
+
+// The device bytes mav1cu_session_create allocates for this geometry: the
+// same list of allocations, summed (checked against the count of a real
+// session by the GPU tests).
+static int64_t session_bytes(const Geometry &g, int maxPresets) {
+  size_t fb = g.frame_bytes, nsb = (size_t)g.num_sbs, mi = (size_t)g.mi_rows * g.mi_cols;
+  size_t plane = (size_t)g.w * g.h, dplane = (size_t)((g.w + 3) >> 2) * ((g.h + 3) >> 2);
+  size_t nblk = (size_t)MAX_BLOCKS_PER_SB * nsb;
+  size_t lrUnits = 3 * (size_t)(g.sb_rows + 1) * (g.sb_cols + 1);
+  size_t b = 6 * fb;                                                   // SRC REC REF GOLD DBK LROUT
+  b += sizeof(FrameParams) + sizeof(int32_t) * 4096 * 15;             // PARAMS MATS
+  b += 2 * sizeof(int32_t) * 2 * NUM_NODES * nsb;                      // MVFIELD MVGOLD
+  b += sizeof(BlockInfo) * MAX_BLOCKS_PER_SB * nsb + sizeof(SbInfo) * nsb + sizeof(int32_t) * COEFS_PER_SB * nsb;
+  b += mi + fb * (maxPresets ? maxPresets : 1) + nsb;                 // LFMASK CDEFBUF CDEF_CHOICE
+  b += sizeof(LrUnit) * lrUnits;                                       // LRUNITS
+  b += (sizeof(int64_t) + sizeof(BlockInfo)) * A_ITEMS * nsb;          // ACOSTS AINFOS
+  b += 2 * 16 * plane + 3 * dplane + 2 * mi;                           // quarter-pel, decimated, edge marks
+  b += sizeof(int) * (nsb + 8 + mi) + sizeof(int32_t) * 4096 * 15;     // waves, status, block map, mats_t
+  b += sizeof(int) * nblk * (4 + MAX_SUCC);                            // ready queue state
+  b += sizeof(int) * MAX_BLOCKS_PER_SB * nsb * 3;                      // claim list, completion flags
+  b += sizeof(int4) * nsb + 2 * sizeof(int) * nsb + sizeof(int) * 4;   // export scratch
+  b += sizeof(lrs::Fit) * lrUnits + sizeof(int) * 4;                   // LR search
+  return (int64_t)b;
+}
+
+extern "C" int64_t mav1cu_session_device_bytes(const mav1cu_session *s) { return s->device_bytes; }
+
 extern "C" int mav1cu_session_create(int width, int height, int max_cdef_presets, mav1cu_session **out, char *err,
                                      size_t errlen) {
   *out = NULL;
@@ -306,37 +342,37 @@ extern "C" int mav1cu_session_create(int width, int height, int max_cdef_presets
   s->size[MAV1CU_BUF_AINFOS] = sizeof(BlockInfo) * A_ITEMS * nsb;
   cudaError_t e = cudaSuccess;
   for (int i = 0; i < MAV1CU_BUF_COUNT && e == cudaSuccess; i++) {
-    e = cudaMalloc(&s->buf[i], s->size[i]);
+    e = dmalloc(s, (void **)&s->buf[i], s->size[i]);
     if (e == cudaSuccess) e = cudaMemset(s->buf[i], 0, s->size[i]);
   }
   size_t plane = (size_t)width * height, dplane = (size_t)((width + 3) >> 2) * ((height + 3) >> 2);
-  if (e == cudaSuccess) e = cudaMalloc(&s->qp[0], 16 * plane);
-  if (e == cudaSuccess) e = cudaMalloc(&s->qp[1], 16 * plane);
-  if (e == cudaSuccess) e = cudaMalloc(&s->dsrc, dplane);
-  if (e == cudaSuccess) e = cudaMalloc(&s->dref[0], dplane);
-  if (e == cudaSuccess) e = cudaMalloc(&s->dref[1], dplane);
-  if (e == cudaSuccess) e = cudaMalloc(&s->ys, (size_t)g.mi_rows * g.mi_cols);
-  if (e == cudaSuccess) e = cudaMalloc(&s->uvs, (size_t)g.mi_rows * g.mi_cols);
-  if (e == cudaSuccess) e = cudaMalloc(&s->waves, sizeof(int) * nsb);
-  if (e == cudaSuccess) e = cudaMalloc(&s->status, sizeof(int) * 8);
-  if (e == cudaSuccess) e = cudaMalloc(&s->blk_at, sizeof(int) * g.mi_rows * g.mi_cols);
-  if (e == cudaSuccess) e = cudaMalloc(&s->mats_t, sizeof(int32_t) * 4096 * 15);
+  if (e == cudaSuccess) e = dmalloc(s, (void **)&s->qp[0], 16 * plane);
+  if (e == cudaSuccess) e = dmalloc(s, (void **)&s->qp[1], 16 * plane);
+  if (e == cudaSuccess) e = dmalloc(s, (void **)&s->dsrc, dplane);
+  if (e == cudaSuccess) e = dmalloc(s, (void **)&s->dref[0], dplane);
+  if (e == cudaSuccess) e = dmalloc(s, (void **)&s->dref[1], dplane);
+  if (e == cudaSuccess) e = dmalloc(s, (void **)&s->ys, (size_t)g.mi_rows * g.mi_cols);
+  if (e == cudaSuccess) e = dmalloc(s, (void **)&s->uvs, (size_t)g.mi_rows * g.mi_cols);
+  if (e == cudaSuccess) e = dmalloc(s, (void **)&s->waves, sizeof(int) * nsb);
+  if (e == cudaSuccess) e = dmalloc(s, (void **)&s->status, sizeof(int) * 8);
+  if (e == cudaSuccess) e = dmalloc(s, (void **)&s->blk_at, sizeof(int) * g.mi_rows * g.mi_cols);
+  if (e == cudaSuccess) e = dmalloc(s, (void **)&s->mats_t, sizeof(int32_t) * 4096 * 15);
   size_t nblk = MAX_BLOCKS_PER_SB * nsb;
-  if (e == cudaSuccess) e = cudaMalloc(&s->dep_count, sizeof(int) * nblk);
-  if (e == cudaSuccess) e = cudaMalloc(&s->succ_count, sizeof(int) * nblk);
-  if (e == cudaSuccess) e = cudaMalloc(&s->succ, sizeof(int) * nblk * MAX_SUCC);
-  if (e == cudaSuccess) e = cudaMalloc(&s->queue, sizeof(int) * nblk);
-  if (e == cudaSuccess) e = cudaMalloc(&s->corners, sizeof(int) * nblk);
+  if (e == cudaSuccess) e = dmalloc(s, (void **)&s->dep_count, sizeof(int) * nblk);
+  if (e == cudaSuccess) e = dmalloc(s, (void **)&s->succ_count, sizeof(int) * nblk);
+  if (e == cudaSuccess) e = dmalloc(s, (void **)&s->succ, sizeof(int) * nblk * MAX_SUCC);
+  if (e == cudaSuccess) e = dmalloc(s, (void **)&s->queue, sizeof(int) * nblk);
+  if (e == cudaSuccess) e = dmalloc(s, (void **)&s->corners, sizeof(int) * nblk);
   s->mats_dirty = 1;
-  if (e == cudaSuccess) e = cudaMalloc(&s->blk_list, sizeof(int) * MAX_BLOCKS_PER_SB * nsb);
-  if (e == cudaSuccess) e = cudaMalloc(&s->blk_done, 2 * sizeof(int) * MAX_BLOCKS_PER_SB * nsb);
-  if (e == cudaSuccess) e = cudaMalloc(&s->xcounts, sizeof(int4) * nsb);
-  if (e == cudaSuccess) e = cudaMalloc(&s->xblk_base, sizeof(int) * nsb);
-  if (e == cudaSuccess) e = cudaMalloc(&s->xcoef_base, sizeof(int) * nsb);
-  if (e == cudaSuccess) e = cudaMalloc(&s->xmeta, sizeof(int) * 4);
+  if (e == cudaSuccess) e = dmalloc(s, (void **)&s->blk_list, sizeof(int) * MAX_BLOCKS_PER_SB * nsb);
+  if (e == cudaSuccess) e = dmalloc(s, (void **)&s->blk_done, 2 * sizeof(int) * MAX_BLOCKS_PER_SB * nsb);
+  if (e == cudaSuccess) e = dmalloc(s, (void **)&s->xcounts, sizeof(int4) * nsb);
+  if (e == cudaSuccess) e = dmalloc(s, (void **)&s->xblk_base, sizeof(int) * nsb);
+  if (e == cudaSuccess) e = dmalloc(s, (void **)&s->xcoef_base, sizeof(int) * nsb);
+  if (e == cudaSuccess) e = dmalloc(s, (void **)&s->xmeta, sizeof(int) * 4);
   s->max_lr_units = 3 * (g.sb_rows + 1) * (g.sb_cols + 1);
-  if (e == cudaSuccess) e = cudaMalloc(&s->lrfit, sizeof(lrs::Fit) * s->max_lr_units);
-  if (e == cudaSuccess) e = cudaMalloc(&s->lr_types, sizeof(int) * 4);
+  if (e == cudaSuccess) e = dmalloc(s, (void **)&s->lrfit, sizeof(lrs::Fit) * s->max_lr_units);
+  if (e == cudaSuccess) e = dmalloc(s, (void **)&s->lr_types, sizeof(int) * 4);
   if (e == cudaSuccess) e = cudaMemset(s->lr_types, 0, sizeof(int) * 4);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->own_stream, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->xs, cudaStreamNonBlocking);
@@ -457,6 +493,7 @@ extern "C" int mav1cu_set_params(mav1cu_session *s, const mav1cu_frame_params *f
     return set_error(s, MAV1CU_ERR_ARG, "frame parameters do not match the session geometry");
   s->fp = *fp;
   s->have_params = 1;
+  s->lr_searched = 0;
   if (s->wave_tile_w != fp->tile_w_sb && build_waves(s, fp->tile_w_sb)) return s->err;
   // by value through a launch: asynchronous for any caller memory (a copy
   // from pageable memory may wait for the stream's earlier work)
@@ -584,6 +621,9 @@ extern "C" int mav1cu_recon(mav1cu_session *s) {
   c.status = s->status;
   c.blk_at = s->blk_at;
   c.done = s->blk_done;
+  c.spin_limit = s->fault_spins > 0 ? s->fault_spins : SPIN_LIMIT;
+  c.hold = s->fault_spins > 0 ? s->fault_hold : -1;
+  s->fault_spins = 0;
   int nsb = s->g.num_sbs;
   if (check_cuda(s, cudaMemsetAsync(s->blk_done, 0, 2 * sizeof(int) * MAX_BLOCKS_PER_SB * nsb, s->stream),
                  "recon flags"))
@@ -619,6 +659,14 @@ extern "C" int mav1cu_recon(mav1cu_session *s) {
   q.next = s->status + 2;
   rec::k_recon_blocks<<<s->resident_recon, rec::INTRA_THREADS, rec::SMEM_INTRA, s->stream>>>(c, q);
   return after_launch(s, "recon intra blocks");
+}
+
+extern "C" int mav1cu_debug_recon_fault(mav1cu_session *s, int hold_block, int spin_limit) {
+  if (spin_limit <= 0 || hold_block < 0 || hold_block >= s->g.num_sbs * MAX_BLOCKS_PER_SB)
+    return set_error(s, MAV1CU_ERR_ARG, "recon fault: block %d, limit %d", hold_block, spin_limit);
+  s->fault_hold = hold_block;
+  s->fault_spins = spin_limit;
+  return MAV1CU_OK;
 }
 
 extern "C" int mav1cu_frame_core(mav1cu_session *s) {
@@ -689,6 +737,7 @@ extern "C" int mav1cu_lr_search(mav1cu_session *s, int lr_test) {
   int n = lr_units_of(s->fp);
   if (n <= 0 || n > s->max_lr_units) return set_error(s, MAV1CU_ERR_ARG, "loop-restoration search: %d units", n);
   export_fence(s);  // LRUNITS and the plane types are exported
+  s->lr_searched = 1;
   lrs::k_lr_fit<<<n, lrs::THREADS, sizeof(lrs::Shared), s->stream>>>(DP(s), U8(s, MAV1CU_BUF_REC),
                                                                        U8(s, MAV1CU_BUF_DBK), U8(s, MAV1CU_BUF_SRC),
                                                                        s->lrfit);
@@ -759,7 +808,7 @@ extern "C" int mav1cu_export(mav1cu_session *s, void *image, size_t cap, int fla
   layout.seq = ++s->xseq;
   int withRec = flags & MAV1CU_EXPORT_REC;
   layout.rec_bytes = withRec ? (int64_t)i420_bytes(s->g) : 0;
-  layout.lr_units = (flags & MAV1CU_EXPORT_LR) ? lr_units_of(s->fp) : 0;
+  layout.lr_units = (flags & MAV1CU_EXPORT_LR) && s->lr_searched ? lr_units_of(s->fp) : 0;
   if (layout.lr_units < 0 || layout.lr_units > s->max_lr_units)
     return set_error(s, MAV1CU_ERR_ARG, "export: %d loop-restoration units", layout.lr_units);
   size_t nsb = (size_t)s->g.num_sbs;
@@ -950,6 +999,7 @@ struct mav1cu_stream {
   cudaEvent_t up_done[NUM_ENGINES][2], load_done[NUM_ENGINES][2];
   int up_next[NUM_ENGINES];
   uint8_t *slot[8];
+  int64_t device_bytes;               // slots and staging (the engines count their own)
   EventRef written[8];                // last write of each slot
   std::vector<EventRef> readers[8];   // reference copies of the slot's picture since then
   size_t i420_bytes;
@@ -973,11 +1023,13 @@ extern "C" int mav1cu_stream_create(const mav1cu_config *cfg, mav1cu_stream **ou
   cudaError_t e = cudaSuccess;
   for (int k = 0; k < 8 && e == cudaSuccess; k++) {
     e = cudaMalloc(&st->slot[k], fb);
+    if (e == cudaSuccess) st->device_bytes += (int64_t)fb;
     if (e == cudaSuccess) e = cudaMemset(st->slot[k], 0, fb);
   }
   for (int k = 0; k < NUM_ENGINES && e == cudaSuccess; k++) {
     for (int b = 0; b < 2 && e == cudaSuccess; b++) {
       e = cudaMalloc(&st->staging[k][b], st->i420_bytes);
+      if (e == cudaSuccess) st->device_bytes += (int64_t)st->i420_bytes;
       if (e == cudaSuccess) e = cudaEventCreateWithFlags(&st->up_done[k][b], cudaEventDisableTiming);
       if (e == cudaSuccess) e = cudaEventCreateWithFlags(&st->load_done[k][b], cudaEventDisableTiming);
     }
@@ -1017,6 +1069,31 @@ extern "C" void mav1cu_stream_destroy(mav1cu_stream *st) {
 }
 
 extern "C" mav1cu_session *mav1cu_stream_session(mav1cu_stream *st) { return st->eng[st->last_engine]; }
+
+extern "C" int mav1cu_stream_reconfigure(mav1cu_stream *st, const mav1cu_config *cfg) {
+  if (!cfg || cfg->width != st->n.c.width || cfg->height != st->n.c.height) return MAV1CU_ERR_ARG;
+  int rc = mav1cu_stream_synchronize(st);
+  if (rc) return rc;
+  st->n = drv::normalise(cfg);
+  for (int k = 0; k < 8; k++) {
+    st->written[k].reset();
+    st->readers[k].clear();
+  }
+  return MAV1CU_OK;
+}
+
+extern "C" int64_t mav1cu_stream_device_bytes(const mav1cu_stream *st) {
+  int64_t b = st->device_bytes;
+  for (int k = 0; k < NUM_ENGINES; k++) b += st->eng[k]->device_bytes;
+  return b;
+}
+
+extern "C" int64_t mav1cu_stream_bytes_for(const mav1cu_config *cfg) {
+  if (!cfg || cfg->width < 16 || cfg->height < 16 || cfg->width > 65536 || cfg->height > 65536) return -1;
+  Geometry g = make_geometry(cfg->width, cfg->height);
+  int64_t i420 = (int64_t)cfg->width * cfg->height + 2 * (int64_t)((cfg->width + 1) >> 1) * ((cfg->height + 1) >> 1);
+  return NUM_ENGINES * session_bytes(g, 4) + 8 * (int64_t)g.frame_bytes + NUM_ENGINES * 2 * i420;
+}
 extern "C" mav1cu_session *mav1cu_stream_engine(mav1cu_stream *st, int k) {
   return k >= 0 && k < NUM_ENGINES ? st->eng[k] : NULL;
 }

@@ -564,6 +564,15 @@ static void frame_done(Job *j) {
   free(tile);
   if (e->dump_path) j->dump = mh_writer_dump_record(w, total, &j->dump_size);
   mh_writer_stats(w, &j->st.num_blocks, &j->st.num_inter_blocks, j->st.tool_use);
+  {
+    /* the LR search's unit counts (lr_select, lr_search.c:350-351) */
+    const mav1cu_export_header *hx = (const mav1cu_export_header *)j->img->image;
+    const mav1cu_lr_unit *lu = (const mav1cu_lr_unit *)(j->img->image + hx->lr_off);
+    for (int k = 0; k < hx->lr_units; k++) {
+      j->st.tool_use[9] += lu[k].type == 1;  /* RESTORE_WIENER */
+      j->st.tool_use[10] += lu[k].type == 2; /* RESTORE_SGRPROJ */
+    }
+  }
   /* the reconstruction section holds the picture as mav1_get_recon returns it */
   const mav1cu_export_header *h = (const mav1cu_export_header *)j->img->image;
   j->recon = malloc(sizeof(Recon) + e->i420);
@@ -597,9 +606,13 @@ static void run_task(Task t) {
       return;
     }
     const uint8_t *img = j->img->image;
+    /* the frame's parameters as the device used them: lr_type is the loop-
+     * restoration search's */
+    memcpy(&j->fp, img + h->params_off, sizeof j->fp);
     mh_frame f = {&j->job, &j->fp, e->low_delay, j->last_hint, j->arf_hint, {0},
                   (const mav1cu_sb_info *)(img + h->sbs_off), (const mav1cu_block_info *)(img + h->blocks_off),
-                  (const int32_t *)(img + h->coefs_off), (const int8_t *)(img + h->cdef_off), NULL};
+                  (const int32_t *)(img + h->coefs_off), (const int8_t *)(img + h->cdef_off),
+                  h->lr_units > 0 ? (const mav1cu_lr_unit *)(img + h->lr_off) : NULL};
     memcpy(f.ref_hint, j->ref_hint, sizeof f.ref_hint);
     mh_writer_frame(j->img->w, &f);
     mh_writer_begin(j->img->w);
@@ -655,7 +668,8 @@ static int submit(struct Mav1Encoder *e, const mav1cu_frame_job *job) {
   if (!j->src) return fail(e, "source frame missing");
   if (mav1cu_stream_encode(e->st, job, j->src, 0)) return fail(e, "stream encode");
   j->sess = mav1cu_stream_engine(e->st, ei);
-  if (mav1cu_export(j->sess, m->image, e->cap, MAV1CU_EXPORT_REC)) return fail(e, "export");
+  if (mav1cu_export(j->sess, m->image, e->cap, MAV1CU_EXPORT_REC | (e->L.cfg.restoration ? MAV1CU_EXPORT_LR : 0)))
+    return fail(e, "export");
   j->seq = mav1cu_export_seq(j->sess);
   atomic_store(&j->state, 1);
   pthread_mutex_lock(&e->mu);
@@ -793,6 +807,57 @@ void mav1_get_recon(const Mav1Encoder *e, uint8_t *const planes[3], const int st
 }
 
 const Mav1FrameStats *mav1_last_stats(const Mav1Encoder *e) { return &e->last; }
+
+int64_t mav1_cuda_device_bytes(const Mav1Encoder *e) { return mav1cu_stream_device_bytes(e->st); }
+
+int mav1_cuda_restart(Mav1Encoder *e, const Mav1Config *cfg) {
+  if (cfg->width != e->cfg.width || cfg->height != e->cfg.height || !cfg->use_metal) return -1;
+  pthread_mutex_lock(&e->mu);
+  while (e->written < e->submitted) pthread_cond_wait(&e->cv, &e->mu);
+  pthread_mutex_unlock(&e->mu);
+  mav1cu_config c;
+  memcpy(&c, cfg, sizeof c);
+  if (mav1cu_stream_reconfigure(e->st, &c)) return fail(e, "restart");
+  e->cfg = *cfg;
+  e->ccfg = c;
+  mav1cu_layout_of(&e->ccfg, &e->L);
+  e->low_delay = e->L.cfg.altref == 0;
+  mh_writer_config(e->hw, &e->L);
+  for (int i = 0; i < e->nimg; i++) mh_writer_config(e->imgs[i].w, &e->L);
+  memset(&e->pl, 0, sizeof e->pl);
+  pthread_mutex_lock(&e->mu);
+  for (int i = 0; i < SRCRING; i++)
+    if (e->srcs[i]) {
+      src_put(e, e->srcs[i]);
+      e->srcs[i] = NULL;
+    }
+  pthread_mutex_unlock(&e->mu);
+  for (int i = e->out_pos; i < e->out_n; i++) {
+    free(e->outq[i].data);
+    recon_unref(e->outq[i].recon);
+  }
+  e->out_pos = e->out_n = 0;
+  free(e->tu);
+  e->tu = NULL;
+  e->tu_pos = e->tu_cap = 0;
+  e->tu_open = 0;
+  for (int k = 0; k < 8; k++) {
+    recon_unref(e->slot_recon[k]);
+    e->slot_recon[k] = NULL;
+  }
+  memset(e->slot_hint, 0, sizeof e->slot_hint);
+  recon_unref(e->shown_recon);
+  e->shown_recon = NULL;
+  memset(&e->last, 0, sizeof e->last);
+  e->flushing = 0;
+  return 0;
+}
+
+int64_t mav1_cuda_device_bytes_for(const Mav1Config *cfg) {
+  mav1cu_config c;
+  memcpy(&c, cfg, sizeof c);
+  return mav1cu_stream_bytes_for(&c);
+}
 
 void mav1_cuda_get_counters(const Mav1Encoder *e, mav1_cuda_counters *out) {
   pthread_mutex_lock((pthread_mutex_t *)&e->mu);

@@ -36,6 +36,8 @@ typedef struct {
  * the writer view); NULL on allocation failure. */
 mh_writer *mh_writer_new(const mav1cu_layout *layout);
 void mh_writer_free(mh_writer *w);
+/* Takes a new configuration of the same frame size (a restarted encoder). */
+void mh_writer_config(mh_writer *w, const mav1cu_layout *layout);
 /* Points the context at a frame: fills the frame header (FrameHdr) the way
  * the reference driver does (alt_code, encoder.c:1004-1030; mav1_encode,
  * encoder.c:822-846; setup_params' header fields, encoder.c:467-509). */

@@ -83,6 +83,11 @@ mh_writer *mh_writer_new(const mav1cu_layout *L) {
   return w;
 }
 
+void mh_writer_config(mh_writer *w, const mav1cu_layout *L) {
+  memcpy(&w->e.cfg, &L->cfg, sizeof w->e.cfg);
+  w->e.leafopt_cfg = L->leafopt_cfg;
+}
+
 void mh_writer_free(mh_writer *w) {
   if (!w) return;
   free(w->e.mi);

@@ -26,7 +26,7 @@ EXPORTS = ["mav1_default_config", "mav1_create", "mav1_encode", "mav1_send_frame
            "mav1_receive_packet_wait", "mav1_pending_packets", "mav1_busy", "mav1_sequence_header", "mav1_get_recon",
            "mav1_last_stats", "mav1_backend_name", "mav1_tool_names", "mav1_destroy",
            # include/mav1_cuda.h
-           "mav1_cuda_get_counters"]
+           "mav1_cuda_get_counters", "mav1_cuda_device_bytes", "mav1_cuda_device_bytes_for", "mav1_cuda_restart"]
 
 
 class FrameStats(ctypes.Structure):
@@ -78,6 +78,12 @@ def lib():
         L.mav1_destroy.restype = None
         L.mav1_cuda_get_counters.argtypes = [vp, ctypes.POINTER(Counters)]
         L.mav1_cuda_get_counters.restype = None
+        L.mav1_cuda_device_bytes.argtypes = [vp]
+        L.mav1_cuda_device_bytes.restype = ctypes.c_int64
+        L.mav1_cuda_device_bytes_for.argtypes = [vp]
+        L.mav1_cuda_device_bytes_for.restype = ctypes.c_int64
+        L.mav1_cuda_restart.argtypes = [vp, vp]
+        L.mav1_cuda_restart.restype = i32
         _libc.free.argtypes = [vp]
         _lib = L
     return _lib
@@ -154,6 +160,16 @@ class Encoder:
     def busy(self):
         return self.lib.mav1_busy(self.h_)
 
+    def device_bytes(self):
+        return self.lib.mav1_cuda_device_bytes(self.h_)
+
+    def restart(self, cfg):
+        """A new clip on this encoder (same frame size; device memory kept)."""
+        cfg = np.ascontiguousarray(cfg)
+        if self.lib.mav1_cuda_restart(self.h_, cfg.ctypes.data):
+            raise Mav1Error("mav1_cuda_restart failed")
+        self.cfg = cfg
+
     def close(self):
         if self.h_:
             self.lib.mav1_destroy(self.h_)
@@ -187,6 +203,11 @@ def encode(frames, cfg, recon=True, counters=None):
     finally:
         enc.close()
     return packets, recons
+
+
+def device_bytes_for(cfg):
+    """Device bytes mav1_create would allocate for the configuration."""
+    return lib().mav1_cuda_device_bytes_for(np.ascontiguousarray(cfg).ctypes.data)
 
 
 def code_frames(enc, frames, expect, recon=True, timeout_ms=60000):

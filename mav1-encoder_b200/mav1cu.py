@@ -73,7 +73,7 @@ EXPORTS = [
     "mav1cu_stream_wait", "mav1cu_stream_join", "mav1cu_stream_synchronize", "mav1cu_edge_types_noalloc",
     "mav1cu_export_capacity", "mav1cu_export_image", "mav1cu_export", "mav1cu_lr_search", "mav1cu_plan_frames",
     "mav1cu_layout_of", "mav1cu_export_seq", "mav1cu_export_wait", "mav1cu_export_query", "mav1cu_host_alloc",
-    "mav1cu_host_free",
+    "mav1cu_host_free", "mav1cu_debug_recon_fault", "mav1cu_stream_reconfigure", "mav1cu_stream_device_bytes", "mav1cu_stream_bytes_for", "mav1cu_session_device_bytes",
 ]
 
 
@@ -104,6 +104,8 @@ def load_library(path=LIB_PATH):
         getattr(lib, f).argtypes = [vp]
         getattr(lib, f).restype = i32
     lib.mav1cu_filter.argtypes = [vp, i32]
+    lib.mav1cu_debug_recon_fault.argtypes = [vp, i32, i32]
+    lib.mav1cu_debug_recon_fault.restype = i32
     lib.mav1cu_lr_search.argtypes = [vp, i32]
     lib.mav1cu_lr_search.restype = i32
     lib.mav1cu_cdef_select.argtypes = [vp, i32]

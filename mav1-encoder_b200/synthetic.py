@@ -165,3 +165,33 @@ def write_y4m(path, spec, frames=None):
         for fr in generate(spec, frames):
             f.write(b"FRAME\n")
             f.write(packed(fr))
+
+
+# ---- the batching workload: 16 streams of uneven size ---------------------------------
+# 4 each of 640x360, 1280x720, 1920x1080 and 2560x1440, 60 frames, every stream
+# with its own seed and the 352x288 recipe scaled to its size: pan, rectangle
+# sizes and rectangle count grow with the width ratio (s = width / 352); blur
+# and noise stay. Each stream's quantizer is drawn from {80, 125, 170} by a
+# seeded generator.
+BATCH_SIZES = [(640, 360), (1280, 720), (1920, 1080), (2560, 1440)]
+BATCH_QS = (80, 125, 170)
+
+
+def batch_streams(frames=60, per_size=4, seed=2024):
+    """[(ClipSpec, q)] of the 16-stream batching workload."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for (w, h) in BATCH_SIZES:
+        s = w / 352.0
+        for k in range(per_size):
+            spec = ClipSpec(w, h, frames, seed=int(rng.integers(1, 1 << 30)), blur=3.0, blur_uv=5.0,
+                            pan=(1.25 * s, -0.5 * s), rects=int(round(4 * s)),
+                            rect_size=(int(round(24 * s)), int(round(64 * s))), noise=2.0,
+                            name=f"batch_{w}x{h}_{k}")
+            out.append((spec, int(rng.choice(BATCH_QS))))
+    return out
+
+
+def packed_clip(spec, frames=None):
+    """The clip's frames as one uint8 array [frames, packed I420 bytes]."""
+    return np.stack([np.frombuffer(packed(f), np.uint8) for f in generate(spec, frames)])

@@ -65,6 +65,8 @@ LARGE_CASES = {
     # search, tx depth, switchable / dual filter, CDEF, loop restoration,
     # --altref 16 --golden --tiles 3, ME range 64): its first 3 frames
     "c2_2160p_full_3f": ("c2_2160p", 3, dict(q=90, altref=16, golden=1, tiles=3, me_range=64)),
+    # the whole configuration: 32 frames, the scene cut at frame 16
+    "c2_2160p_full_32f": ("c2_2160p", 32, dict(q=90, altref=16, golden=1, tiles=3, me_range=64)),
 }
 
 
@@ -95,13 +97,41 @@ def run_large(name):
         "recon": h(b"".join(p.tobytes() for r in recons for p in r)),
         "dump": h(dec),
         "packets": len(packets),
+        "packet_sha16": [h(p)[:16] for p in packets],
     }
 
 
+def run_batch():
+    """The 16-stream batching workload (synthetic.batch_streams, --turbo with
+    each stream's q): per stream the hashes of its clip, IVF bitstream and
+    shown reconstructions as the oracle codes it alone."""
+    h = lambda b: hashlib.sha256(b).hexdigest()
+    out = {}
+    for spec, q in synthetic.batch_streams():
+        frames = list(synthetic.generate(spec))
+        packets, recons = oracle.encode(frames, oracle.cli_config(spec.width, spec.height, q=q, turbo=1))
+        out[spec.name] = {
+            "clip": hashlib.sha256(b"".join(synthetic.packed(f) for f in frames)).hexdigest(),
+            "q": q,
+            "ivf": h(oracle.ivf_bytes(packets, spec.width, spec.height)),
+            "recon": h(b"".join(p.tobytes() for r in recons for p in r)),
+            "packets": len(packets),
+        }
+        print(spec.name, out[spec.name]["ivf"][:16], flush=True)
+    return out
+
+
 if __name__ == "__main__":
-    if "--large" in sys.argv:
-        out = {name: run_large(name) for name in LARGE_CASES}
-        json.dump(out, open(os.path.join(HERE, "dropin_hashes.json"), "w"), indent=1, sort_keys=True)
+    if "--batch" in sys.argv:
+        out = run_batch()
+        json.dump(out, open(os.path.join(HERE, "batch_hashes.json"), "w"), indent=1, sort_keys=True)
+    elif "--large" in sys.argv:
+        # --case NAME recomputes one entry and keeps the others
+        names = [sys.argv[sys.argv.index("--case") + 1]] if "--case" in sys.argv else list(LARGE_CASES)
+        path = os.path.join(HERE, "dropin_hashes.json")
+        out = json.load(open(path)) if os.path.exists(path) and "--case" in sys.argv else {}
+        out.update({name: run_large(name) for name in names})
+        json.dump(out, open(path, "w"), indent=1, sort_keys=True)
     else:
         # --case NAME recomputes one entry and keeps the others
         names = [sys.argv[sys.argv.index("--case") + 1]] if "--case" in sys.argv else list(CASES)

@@ -38,6 +38,15 @@ CASES = {
     "lowdelay": (synthetic.ClipSpec(150, 102, 6, seed=32, rects=2, rect_size=(16, 40)), 6,
                  dict(q=200, golden=1, keyint=4, lr=0)),
     "lossless": (synthetic.ClipSpec(96, 64, 3, seed=33, rects=1, rect_size=(16, 32)), 3, dict(q=0, fast=1)),
+    # the full tool set of the 4K configuration (loop restoration included) on an odd-sized clip
+    "full_tools": (synthetic.ClipSpec(203, 131, 9, seed=31, rects=3, rect_size=(16, 48)), 9,
+                   dict(q=90, altref=4, golden=1, tiles=1, me_range=64)),
+    # low delay with lr_test (Wiener and self-guided units forced), q 200
+    "lowdelay_lrtest": (synthetic.ClipSpec(150, 102, 6, seed=32, rects=2, rect_size=(16, 40)), 6,
+                        dict(q=200, golden=1, keyint=4, lr_test=1)),
+    # loop restoration on a wider frame with several tile columns and ALTREF 16
+    "lr_altref16": (synthetic.ClipSpec(640, 360, 20, seed=35, rects=5, rect_size=(32, 96), cut=12), 20,
+                    dict(q=110, altref=16, tiles=2)),
     # the benchmark clip and flags (key, ALTREF, leaf and a second key frame)
     "c1_1080p_turbo": (synthetic.CONFIGS["c1_1080p"], 9, dict(q=125, turbo=1, keyint=8, tiles=2)),
 }
@@ -148,3 +157,37 @@ def test_benchmark_clip_matches_golden():
     assert [i for i, (a, b) in enumerate(zip(got, want["packet_sha16"])) if a != b] == []
     assert _h(mav1api.ivf_bytes(packets, spec.width, spec.height)) == want["ivf"]
     assert _h(b"".join(p.tobytes() for r in recons for p in r)) == want["recon"]
+
+
+def _mg():
+    import importlib.util
+    spec_ = importlib.util.spec_from_file_location("make_golden", os.path.join(HERE, "golden", "make_golden.py"))
+    mg = importlib.util.module_from_spec(spec_)
+    spec_.loader.exec_module(mg)
+    return mg
+
+
+@pytest.mark.parametrize("name", ["c2_2160p_full_3f", "c2_2160p_full_32f"])
+def test_api_full_tools_2160p_matches_golden(name, tmp_path):
+    """The benchmark spec's full-tool configuration at full size (3840x2160,
+    -q 90, tx search, tx depth, switchable / dual filter, CDEF, loop
+    restoration searched on the device, --altref 16 --golden --tiles 3, ME
+    range 64; the first 3 frames, and all 32 with the scene cut at frame 16)
+    through the API, against the oracle's hashes (tests/golden/
+    dropin_hashes.json, written by make_golden.py --large)."""
+    hashes = json.load(open(os.path.join(HERE, "golden", "dropin_hashes.json")))
+    if name not in hashes:
+        pytest.skip(f"no golden hashes for {name}")
+    want = hashes[name]
+    mg = _mg()
+    spec, frames, flags = mg.large_frames(name)
+    assert mg.frames_sha256(frames) == want["frames"]
+    dump = str(tmp_path / "ours.dec")
+    packets, recons = _ours(spec, frames, flags, dump)
+    assert len(packets) == want["packets"]
+    if "packet_sha16" in want:
+        got = [_h(p)[:16] for p in packets]
+        assert [i for i, (a, b) in enumerate(zip(got, want["packet_sha16"])) if a != b] == []
+    assert _h(mav1api.ivf_bytes(packets, spec.width, spec.height)) == want["ivf"]
+    assert _h(b"".join(p.tobytes() for r in recons for p in r)) == want["recon"]
+    assert _h(open(dump, "rb").read()) == want["dump"]
