@@ -489,17 +489,31 @@ def cpu_reference(sample_frames):
     return sample_frames / wall, wall, sample_frames * os.cpu_count() / cpu
 
 
-def profile_run(n):
+def profile_run(n, export=False, lr=False):
+    """Codes the first n planned frames once (a short run for ncu): the
+    benchmark clip, or with lr a 640x360 clip with every tool on (loop
+    restoration searched on the device); with export, every frame's writer
+    inputs and reconstruction are exported into page-locked memory."""
     import torch
     import mav1cu
 
-    frames_host = load_clip(SPEC)
-    cfg = mav1cu.cli_config(SPEC.width, SPEC.height, **FLAGS)
-    jobs = mav1cu.plan(cfg, SPEC.frames)[:n]
+    if lr:
+        spec = synthetic.ClipSpec(640, 360, n, seed=35, rects=5, rect_size=(32, 96))
+        frames_host = np.stack([np.frombuffer(synthetic.packed(f), np.uint8) for f in synthetic.generate(spec)])
+        cfg = mav1cu.cli_config(spec.width, spec.height, q=110, altref=4, tiles=2)
+    else:
+        spec = SPEC
+        frames_host = load_clip(SPEC)
+        cfg = mav1cu.cli_config(SPEC.width, SPEC.height, **FLAGS)
+    jobs = mav1cu.plan(cfg, spec.frames)[:n]
     st = mav1cu.Stream(cfg)
     frames_dev = torch.from_numpy(frames_host[: max(j["disp"] for j in jobs) + 1]).cuda()
+    image = torch.empty(st.session.export_capacity(), dtype=torch.uint8).pin_memory() if export else None
     for j in jobs:
-        st.encode(j, frames_dev[j["disp"]].data_ptr(), True)
+        sess = st.encode(j, frames_dev[j["disp"]].data_ptr(), True)
+        if export:
+            sess.export(image.data_ptr(), image.numel(), rec=True)
+            st.synchronize()
     st.synchronize()
     print(json.dumps({"profile_frames": n, "kinds": [int(j["kind"]) for j in jobs], "launches": int(st.launches())}))
     st.close()
@@ -521,9 +535,12 @@ def main():
     ap.add_argument("--serving-sessions", type=int, default=400)
     ap.add_argument("--profile-frames", type=int, default=0,
                     help="code the clip's first N planned frames once and exit (a short run for ncu)")
+    ap.add_argument("--profile-export", action="store_true", help="with --profile-frames: export every frame")
+    ap.add_argument("--profile-lr", action="store_true",
+                    help="with --profile-frames: a 640x360 clip with every tool on (loop restoration)")
     args = ap.parse_args()
     if args.profile_frames:
-        profile_run(args.profile_frames)
+        profile_run(args.profile_frames, export=args.profile_export, lr=args.profile_lr)
         return
     if args.workload == "serving":
         import torch

@@ -41,31 +41,54 @@ HD int dec_h(const FrameParams *fp) { return (fp->frame_h + 3) >> 2; }
 
 // Plane fy * 4 + fx holds the EIGHTTAP prediction of (y + fy / 4, x + fx / 4)
 // (k_me.h:289-313): horizontal Round2( ., 3 ), vertical Round2( ., 11 ), Clip1.
-__global__ void k_qpel_planes(const FrameParams *fp, const uint8_t *ref, uint8_t *qp) {
-  int W = fp->frame_w, H = fp->frame_h;
-  int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
-  if (x >= W || y >= H) return;
+// A CTA of 32 x 8 threads makes a QP_TW x QP_TH tile of all 16 planes: the
+// clamped reference window (QP_TH + 7 rows, QP_TW + 7 columns) is staged in
+// shared memory once, the horizontal pass (4 phases) runs once per window
+// row and column, and each thread forms 4 consecutive samples of one row for
+// every plane, stored as one 32-bit word where the plane row allows. Every
+// sample is the same sums and roundings as the per-sample definition.
+constexpr int QP_TW = 128, QP_TH = 8, QP_THREADS = 256;
+
+__global__ void __launch_bounds__(QP_THREADS) k_qpel_planes(const FrameParams *fp, const uint8_t *ref, uint8_t *qp) {
+  __shared__ uint8_t win[QP_TH + 7][QP_TW + 8];
+  __shared__ int16_t hs[4][QP_TH + 7][QP_TW];
+  const int W = fp->frame_w, H = fp->frame_h, stride = fp->stride[0];
   const uint8_t *rp = ref + fp->offset[0];
-  int stride = fp->stride[0];
-  int hrow[4][8];
-  for (int t = 0; t < 8; t++) {
-    const uint8_t *row = rp + clip3(0, H - 1, y + t - 3) * stride;
+  const int x0 = blockIdx.x * QP_TW, y0 = blockIdx.y * QP_TH, tid = threadIdx.x;
+  for (int i = tid; i < (QP_TH + 7) * (QP_TW + 7); i += QP_THREADS) {
+    int r = i / (QP_TW + 7), c = i - r * (QP_TW + 7);
+    win[r][c] = rp[clip3(0, H - 1, y0 + r - 3) * stride + clip3(0, W - 1, x0 + c - 3)];
+  }
+  __syncthreads();
+  for (int i = tid; i < (QP_TH + 7) * QP_TW; i += QP_THREADS) {
+    int r = i / QP_TW, x = i - r * QP_TW;
     int px[8];
-    for (int u = 0; u < 8; u++) px[u] = row[clip3(0, W - 1, x + u - 3)];
+    for (int u = 0; u < 8; u++) px[u] = win[r][x + u];
     for (int fx = 0; fx < 4; fx++) {
       const int32_t *f = d_Subpel_Filters[EIGHTTAP][4 * fx];
-      int s = 0;
-      for (int u = 0; u < 8; u++) s += f[u] * px[u];
-      hrow[fx][t] = round2(s, 3);
+      int sum = 0;
+      for (int u = 0; u < 8; u++) sum += f[u] * px[u];
+      hs[fx][r][x] = (int16_t)round2(sum, 3);
     }
   }
-  size_t o = (size_t)y * W + x, n = (size_t)W * H;
+  __syncthreads();
+  const int ty = tid >> 5, xx = (tid & 31) * 4, y = y0 + ty, x = x0 + xx;
+  if (y >= H || x >= W) return;
+  const size_t n = (size_t)W * H, o = (size_t)y * W + x;
+  const bool word = (W & 3) == 0 && x + 3 < W;  // 4-byte aligned and inside the row
   for (int fy = 0; fy < 4; fy++) {
     const int32_t *f = d_Subpel_Filters[EIGHTTAP][4 * fy];
     for (int fx = 0; fx < 4; fx++) {
-      int s = 0;
-      for (int t = 0; t < 8; t++) s += f[t] * hrow[fx][t];
-      qp[(size_t)(fy * 4 + fx) * n + o] = (uint8_t)clip1(round2(s, 11));
+      uint32_t packed = 0;
+      uint8_t *plane = qp + (size_t)(fy * 4 + fx) * n;
+      for (int k = 0; k < 4; k++) {
+        int sum = 0;
+        for (int t = 0; t < 8; t++) sum += f[t] * hs[fx][ty + t][xx + k];
+        uint32_t v = (uint32_t)clip1(round2(sum, 11));
+        if (word) packed |= v << (8 * k);
+        else if (x + k < W) plane[o + k] = (uint8_t)v;
+      }
+      if (word) *(uint32_t *)(plane + o) = packed;
     }
   }
 }

@@ -8,25 +8,30 @@
 // the normative inverse transform added back into `rec`; optional luma
 // transform-type search and intra tx_depth search by 16 * SSE + lambda * bits.
 //
-// B200 mapping: one launch per frame codes every block, one warp (a CTA of
-// 32 threads) per block. Blocks are claimed from a list in superblock wave
-// order ((c - tileStart) + 2r), decode order inside a superblock: a
-// topological order of the sample dependencies, so a persistent worker that
-// waits only ever waits on blocks already claimed by running workers. An
-// inter block reads reference pictures only and starts at once. Before
-// each intra transform block the worker waits on the completion flags of
-// exactly the blocks whose samples its edges read (above row to the
-// aboveLimit, left column to the leftLimit, spec 7.11.2), so the critical
-// path follows the block-level wavefront instead of whole superblocks.
-// BlockDecoded availability is a function of the decode order: a unit of
-// the superblock is decoded when the block covering it precedes this one
-// (a map from 4x4 units to block indices), or by the clear-flags rule
-// (k_recon.h:402-414) outside the superblock. Samples of the frame being
-// written are read through L2 (ldpx), as other SMs write them during the
-// launch. Within a transform block the warp splits the residual, both
-// matrix passes (64-bit accumulation), the quantiser, the eob search (a max
-// over inverse-scan positions), the row / column inverse kernels and the
-// reconstruction.
+// B200 mapping, two launches per frame:
+//  - k_recon_inter: a 128-thread CTA per superblock codes its inter blocks
+//    (they read reference pictures only, so every superblock starts at once)
+//    and publishes each block's completion flags;
+//  - k_recon_blocks: the intra blocks as dataflow. A prepass (k_block_map,
+//    k_block_order, k_block_deps) maps every 4x4 unit to its block, lists the
+//    intra blocks, and gives each one its dependency count (the intra blocks
+//    under its luma edge samples, spec 7.11.2 aboveLimit / leftLimit), its
+//    place in those blocks' successor lists and the BlockDecoded bits of its
+//    corner units; blocks without dependencies seed a ready queue. Persistent
+//    128-thread workers (at most one per SM, max(8, intra blocks / 8) of
+//    them) pop ready blocks, stage each one in shared memory in one batch of
+//    copies, code its luma, write it back, publish its luma flag and release
+//    its successors (the last release pushes a successor to the queue), then
+//    wait (bounded) on the chroma flags under its chroma edges and code its
+//    chroma. Every wait is bounded (Ctx::spin_limit polls); past it the
+//    worker sets the error and abort words and every worker stops.
+// BlockDecoded availability is a function of the decode order (the unit map
+// and the corner bits) or of the clear-flags rule (k_recon.h:402-414)
+// outside the superblock. Samples of the frame being written are read
+// through L2 (ldpx), as other SMs write them during the launch. Within a
+// transform block the CTA splits the residual, both matrix passes (64-bit
+// accumulation), the quantiser, the eob search (a max over inverse-scan
+// positions), the row / column inverse kernels and the reconstruction.
 #pragma once
 
 #include "common.cuh"

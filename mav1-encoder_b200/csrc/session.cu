@@ -11,6 +11,7 @@
 #include <string.h>
 
 #include <memory>
+#include <mutex>
 #include <vector>
 
 #include "common.cuh"
@@ -212,7 +213,11 @@ static int upload_inverse_scans(mav1cu_session *s) {
 // are identical (checked against the reference's table by the tests).
 static void build_fwd_one(int kind, int log2n, int32_t *out) {
   int n = 1 << log2n, m = n > 32 ? 32 : n;
-  static double A[64][32], M[32][32 + 64];
+  // working arrays of this call (sessions may be created from several host
+  // threads at once)
+  std::vector<double> Av(64 * 32), Mv(32 * (32 + 64));
+  double(*A)[32] = (double(*)[32])Av.data();
+  double(*M)[32 + 64] = (double(*)[32 + 64])Mv.data();
   const double S = 65536.0;
   for (int j = 0; j < m; j++) {
     int32_t t[64];
@@ -251,7 +256,7 @@ static void build_fwd_one(int kind, int log2n, int32_t *out) {
     for (int i = 0; i < n; i++) out[k * n + i] = (int32_t)lrint(M[k][m + i] * (double)(1 << 20));
 }
 
-extern "C" void mav1cu_build_fwd_matrices(int32_t *mats) {
+static void build_fwd_all(int32_t *mats) {
   memset(mats, 0, sizeof(int32_t) * 4096 * 15);
   for (int kind = 0; kind < 3; kind++)
     for (int log2n = 2; log2n <= 6; log2n++) {
@@ -259,6 +264,14 @@ extern "C" void mav1cu_build_fwd_matrices(int32_t *mats) {
       if (kind == tx::KIND_IDTX && log2n > 5) continue;
       build_fwd_one(kind, log2n, mats + rec::fwd_slot(kind, log2n));
     }
+}
+
+// The table is a constant of the transforms: derived once per process.
+extern "C" void mav1cu_build_fwd_matrices(int32_t *mats) {
+  static std::vector<int32_t> table(4096 * 15);
+  static std::once_flag once;
+  std::call_once(once, [] { build_fwd_all(table.data()); });
+  memcpy(mats, table.data(), sizeof(int32_t) * 4096 * 15);
 }
 
 // ---- session -------------------------------------------------------------------------
@@ -516,9 +529,10 @@ extern "C" int mav1cu_motion_search(mav1cu_session *s) {
   int nref = fp.golden ? 2 : 1;
   const uint8_t *refs[2] = {U8(s, MAV1CU_BUF_REF), U8(s, MAV1CU_BUF_GOLD)};
   if (fp.turbo & T_ME_HPEL) {
-    dim3 blk(128), grid((fp.frame_w + 127) / 128, fp.frame_h);
+    dim3 blk(128);
+    dim3 qgrid((fp.frame_w + me::QP_TW - 1) / me::QP_TW, (fp.frame_h + me::QP_TH - 1) / me::QP_TH);
     for (int r = 0; r < nref; r++) {
-      me::k_qpel_planes<<<grid, blk, 0, s->stream>>>(DP(s), refs[r], s->qp[r]);
+      me::k_qpel_planes<<<qgrid, me::QP_THREADS, 0, s->stream>>>(DP(s), refs[r], s->qp[r]);
       if (after_launch(s, "qpel planes")) return s->err;
     }
     if (fp.turbo & T_ME_DEC) {

@@ -131,3 +131,21 @@ def test_butterfly_sums_fit_32_bits(tmp_path):
                    check=True, capture_output=True)
     r = subprocess.run([str(exe)], capture_output=True, text=True)
     assert r.returncode == 0, r.stdout + r.stderr
+
+
+def test_forward_matrices_identical_from_concurrent_threads():
+    """Sessions are created from several host threads at once (one encoder per
+    thread); the forward-matrix table each one gets must be the same."""
+    import threading
+    want = mav1cu.fwd_matrices()
+    out = [None] * 8
+
+    def one(i):
+        out[i] = [mav1cu.fwd_matrices() for _ in range(4)]
+
+    th = [threading.Thread(target=one, args=(i,)) for i in range(8)]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join()
+    assert all(np.array_equal(m, want) for ms in out for m in ms)
