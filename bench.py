@@ -140,7 +140,6 @@ def batch_bench(args):
     # keyint = clip length: the clip codes as with keyint 0 (one key frame),
     # and a live encoder codes it again as a new closed GOP at every pass
     cfgs = [mav1cu.cli_config(s.width, s.height, q=q, turbo=1, keyint=s.frames) for s, q in specs]
-    os.environ.setdefault("MAV1_CUDA_IMAGES", "3")
     B = batch.Batch(list(zip(cfgs, frames)))
     try:
         want = {}

@@ -51,7 +51,7 @@ constexpr int QP_TW = 128, QP_TH = 8, QP_THREADS = 256;
 
 __global__ void __launch_bounds__(QP_THREADS) k_qpel_planes(const FrameParams *fp, const uint8_t *ref, uint8_t *qp) {
   __shared__ uint8_t win[QP_TH + 7][QP_TW + 8];
-  __shared__ int16_t hs[4][QP_TH + 7][QP_TW];
+  __shared__ __align__(16) int16_t hs[4][QP_TH + 7][QP_TW];
   const int W = fp->frame_w, H = fp->frame_h, stride = fp->stride[0];
   const uint8_t *rp = ref + fp->offset[0];
   const int x0 = blockIdx.x * QP_TW, y0 = blockIdx.y * QP_TH, tid = threadIdx.x;
@@ -76,14 +76,23 @@ __global__ void __launch_bounds__(QP_THREADS) k_qpel_planes(const FrameParams *f
   if (y >= H || x >= W) return;
   const size_t n = (size_t)W * H, o = (size_t)y * W + x;
   const bool word = (W & 3) == 0 && x + 3 < W;  // 4-byte aligned and inside the row
-  for (int fy = 0; fy < 4; fy++) {
-    const int32_t *f = d_Subpel_Filters[EIGHTTAP][4 * fy];
-    for (int fx = 0; fx < 4; fx++) {
-      uint32_t packed = 0;
+  for (int fx = 0; fx < 4; fx++) {
+    // this thread's 8 rows x 4 columns of horizontal sums, one 8-byte load per row
+    int hv[8][4];
+    for (int t = 0; t < 8; t++) {
+      int2 w2 = *(const int2 *)&hs[fx][ty + t][xx];
+      hv[t][0] = (int16_t)(w2.x & 0xffff);
+      hv[t][1] = (int16_t)(w2.x >> 16);
+      hv[t][2] = (int16_t)(w2.y & 0xffff);
+      hv[t][3] = (int16_t)(w2.y >> 16);
+    }
+    for (int fy = 0; fy < 4; fy++) {
+      const int32_t *f = d_Subpel_Filters[EIGHTTAP][4 * fy];
       uint8_t *plane = qp + (size_t)(fy * 4 + fx) * n;
+      uint32_t packed = 0;
       for (int k = 0; k < 4; k++) {
         int sum = 0;
-        for (int t = 0; t < 8; t++) sum += f[t] * hs[fx][ty + t][xx + k];
+        for (int t = 0; t < 8; t++) sum += f[t] * hv[t][k];
         uint32_t v = (uint32_t)clip1(round2(sum, 11));
         if (word) packed |= v << (8 * k);
         else if (x + k < W) plane[o + k] = (uint8_t)v;
