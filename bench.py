@@ -210,6 +210,37 @@ def serving_bench(args, capacity_pxs):
     return res
 
 
+def full4k_bench(args):
+    """The full filter and search chain (3840x2160, 32 frames with a scene cut
+    at frame 16, -q 90, tx search, tx depth, switchable / dual filter, CDEF,
+    loop restoration searched on the device, --altref 16 --golden --tiles 3,
+    ME range 64) through the encoder API from host frames, wall clock per
+    pass; the bitstream is checked against the oracle's hashes
+    (tests/golden/dropin_hashes.json) when they are present."""
+    import batch
+    import mav1api
+    import mav1cu
+
+    spec = synthetic.CONFIGS["c2_2160p"]
+    frames = batch.load_streams([spec])[0]
+    cfg = mav1cu.cli_config(spec.width, spec.height, q=90, altref=16, golden=1, tiles=3, me_range=64)
+    want = json.load(open(os.path.join(ROOT, "tests", "golden", "dropin_hashes.json"))).get("c2_2160p_full_32f")
+    walls, bitexact = [], None
+    for i in range(1 + max(1, args.full4k_passes)):
+        t0 = time.perf_counter()
+        packets, _ = mav1api.encode(list(frames), cfg, recon=False)
+        dt = time.perf_counter() - t0
+        if i == 0:
+            if want:
+                bitexact = hashlib.sha256(mav1api.ivf_bytes(packets, spec.width, spec.height)).hexdigest() == want["ivf"]
+            continue
+        walls.append(dt)
+    return {"workload": "3840x2160 synthetic clip, 32 frames (scene cut at 16), -q 90 --altref 16 --golden --tiles 3 "
+                        "--me-range 64, every tool on (tx search, tx depth, dual filter, CDEF, loop restoration)",
+            "fps": round(spec.frames * len(walls) / sum(walls), 3), "passes": len(walls),
+            "s_per_pass": round(sum(walls) / len(walls), 2), "bitexact_to_oracle": bitexact}
+
+
 def max_over_ranks(values, device):
     """Element-wise maximum of this rank's timings over the process group:
     each replica times its own GPU, and the slowest one defines the step. The
@@ -438,24 +469,47 @@ def kernel_times(sess, stream, frames_dev):
 # (510 x 6144 x 4), forward matrices read (61,440 x 4).
 KEY_RECON_BYTES = 2 * 3133440 + 2 * 510 * 64 * 108 + 510 * 6144 * 4 + 61440 * 4
 # dram__bytes_read.sum + dram__bytes_write.sum of that launch of k_recon_blocks
-# in one ncu capture (the key frame of `bench.py --profile-frames 3`).
-KEY_RECON_DRAM_BYTES = 19850000
+# in one ncu capture (the key frame of `bench.py --profile-frames 3
+# --profile-export`: 18.467 MB read + 1.447 MB written,
+# profiles/k_recon_blocks_1080p_turbo_3frames.md).
+KEY_RECON_DRAM_BYTES = 19914752
+
+
+# Integer-pipe figures of each stage's main kernel from the committed ncu
+# captures (profiles/*_1080p_turbo_3frames.md: the clip's first key, ALTREF
+# and leaf frames): the ALU pipe's share of its peak and the issue slots
+# active, ranges over the captured launches.
+STAGE_NCU = {
+    "motion_search": ("k_me_level", "31-41", "27-47", "profiles/k_me_level_1080p_turbo_3frames.md"),
+    "analyze": ("k_analyze_level", "20-27", "28-37", "profiles/k_analyze_level_1080p_turbo_3frames.md"),
+    "recon": ("k_recon_inter", "18", "26", "profiles/k_recon_inter_1080p_turbo_3frames.md"),
+    "filter": ("k_deblock, k_cdef", "49-59", "63-67", "profiles/k_deblock_1080p_turbo_3frames.md"),
+}
 
 
 def roofline(kern, peaks):
     """Roofline of the dominant kernel (k_recon_blocks) through its stage on
     the key frame: algorithmic bytes over the measured stage time, against the
     measured HBM copy bandwidth. The kernel is a dependency chain (latency
-    bound), so the fraction is small by nature."""
+    bound), so the fraction is small by nature; `stages` gives every stage's
+    live time on an ALTREF frame with its main kernel's integer-pipe
+    utilisation from the committed ncu captures."""
     if not kern:
         return None
     t = kern["key_recon_ms"] * 1e-3
     peak = peaks.get("hbm_gbs", 6650.0)
     achieved = KEY_RECON_BYTES / t / 1e9
+    stages = []
+    for name, ms in kern["arf_stage_ms"].items():
+        ent = {"stage": name, "ms": round(ms, 4)}
+        if name in STAGE_NCU:
+            k, alu, issue, src = STAGE_NCU[name]
+            ent.update({"kernel": k, "alu_pipe_pct_of_peak": alu, "issue_active_pct": issue, "ncu": src})
+        stages.append(ent)
     return {"bound": "hbm", "kernel": "k_recon_blocks (key-frame recon stage)", "achieved": round(achieved, 2),
             "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 6), "traffic": KEY_RECON_DRAM_BYTES,
             "algorithmic_bytes": KEY_RECON_BYTES, "ms_per_launch": round(kern["key_recon_ms"], 3),
-            "arf_stage_ms": {k: round(v, 4) for k, v in kern["arf_stage_ms"].items()},
+            "stages_altref_frame": stages,
             "peak_source": "MEASURED_PEAKS.json" if "hbm_gbs" in peaks else "fallback"}
 
 
@@ -529,8 +583,10 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the 16-stream batching measurement")
     ap.add_argument("--batch-passes", type=int, default=2)
-    ap.add_argument("--workload", default="clip", choices=["clip", "serving"],
-                    help="serving: the session-serving measurement alone (about two minutes)")
+    ap.add_argument("--workload", default="clip", choices=["clip", "serving", "full4k"],
+                    help="serving: the session-serving measurement alone (about two minutes); full4k: the 4K "
+                         "full-tool configuration")
+    ap.add_argument("--full4k-passes", type=int, default=1)
     ap.add_argument("--serving-sessions", type=int, default=400)
     ap.add_argument("--profile-frames", type=int, default=0,
                     help="code the clip's first N planned frames once and exit (a short run for ncu)")
@@ -540,6 +596,11 @@ def main():
     args = ap.parse_args()
     if args.profile_frames:
         profile_run(args.profile_frames, export=args.profile_export, lr=args.profile_lr)
+        return
+    if args.workload == "full4k":
+        import torch
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+        print(json.dumps(full4k_bench(args)))
         return
     if args.workload == "serving":
         import torch

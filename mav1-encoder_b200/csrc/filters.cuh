@@ -385,12 +385,30 @@ HD int lr_src(const FrameParams *fp, int plane, const LrBlock *lb, const uint8_t
   return cdef[fp->offset[plane] + y * stride + x];
 }
 
-// Wiener filter (spec 7.17.4, 8-bit rounding). Each output sample goes to
-// sink(offset in the plane buffer, value): the apply kernel stores it, the
-// parameter search accumulates its squared error.
-template <class Sink>
-HD void lr_wiener_to(const FrameParams *fp, int plane, const LrBlock *lb, const uint8_t *cdef, const uint8_t *dbk,
-                     const LrUnit *u, Sink &sink) {
+// The samples the loop-restoration filters read: get_source_sample( ) for
+// the filter taps, and the CDEF output at the block's own positions. FrameSrc
+// reads the frame buffers; the parameter search reads shared-memory windows
+// (lrs::WinSrc) through the same filter code.
+struct FrameSrc {
+  const FrameParams *fp;
+  int plane;
+  const uint8_t *cdef, *dbk;
+  HD int tap(const LrBlock *lb, int x, int y) const { return lr_src(fp, plane, lb, cdef, dbk, x, y); }
+  HD int own(int x, int y) const { return cdef[fp->offset[plane] + y * fp->stride[plane] + x]; }
+};
+
+// Output of the filters: sink(x, y, value) for plane sample (x, y). The apply
+// kernel stores it, the parameter search accumulates its squared error.
+struct StoreSink {
+  const FrameParams *fp;
+  int plane;
+  uint8_t *out;
+  HD void operator()(int x, int y, int v) { out[fp->offset[plane] + y * fp->stride[plane] + x] = (uint8_t)v; }
+};
+
+// Wiener filter (spec 7.17.4, 8-bit rounding).
+template <class Src, class Sink>
+HD void lr_wiener_to(const LrBlock *lb, const Src &in, const LrUnit *u, Sink &sink) {
   int vf[7], hf[7];
   vf[3] = 128;
   hf[3] = 128;
@@ -407,32 +425,27 @@ HD void lr_wiener_to(const FrameParams *fp, int plane, const LrBlock *lb, const 
   for (int r = 0; r < lb->h + 6; r++)
     for (int c = 0; c < lb->w; c++) {
       int s = 0;
-      for (int t = 0; t < 7; t++) s += hf[t] * lr_src(fp, plane, lb, cdef, dbk, lb->x + c + t - 3, lb->y + r - 3);
+      for (int t = 0; t < 7; t++) s += hf[t] * in.tap(lb, lb->x + c + t - 3, lb->y + r - 3);
       inter[r][c] = clip3(-offset, limit - offset, round2(s, round0));
     }
-  int stride = fp->stride[plane];
   for (int r = 0; r < lb->h; r++)
     for (int c = 0; c < lb->w; c++) {
       int s = 0;
       for (int t = 0; t < 7; t++) s += vf[t] * inter[r + t][c];
-      sink(fp->offset[plane] + (lb->y + r) * stride + lb->x + c, clip3(0, 255, round2(s, round1)));
+      sink(lb->x + c, lb->y + r, clip3(0, 255, round2(s, round1)));
     }
 }
 
-struct StoreSink {
-  uint8_t *out;
-  HD void operator()(int o, int v) { out[o] = (uint8_t)v; }
-};
-
 HD void lr_wiener(const FrameParams *fp, int plane, const LrBlock *lb, const uint8_t *cdef, const uint8_t *dbk,
                   uint8_t *out, const LrUnit *u) {
-  StoreSink sink{out};
-  lr_wiener_to(fp, plane, lb, cdef, dbk, u, sink);
+  FrameSrc in{fp, plane, cdef, dbk};
+  StoreSink sink{fp, plane, out};
+  lr_wiener_to(lb, in, u, sink);
 }
 
 // Box filter (spec 7.17.3); F gets w x h values (row stride 4).
-HD void lr_box(const FrameParams *fp, int plane, const LrBlock *lb, const uint8_t *cdef, const uint8_t *dbk, int set,
-               int pass, int *F) {
+template <class Src>
+HD void lr_box(const LrBlock *lb, const Src &in, int set, int pass, int *F) {
   int r = T(Sgr_Params)[set][pass * 2 + 0];
   if (r == 0) return;
   int eps = T(Sgr_Params)[set][pass * 2 + 1];
@@ -446,7 +459,7 @@ HD void lr_box(const FrameParams *fp, int plane, const LrBlock *lb, const uint8_
       long long a = 0, b = 0;
       for (int dy = -r; dy <= r; dy++)
         for (int dx = -r; dx <= r; dx++) {
-          long long c = lr_src(fp, plane, lb, cdef, dbk, lb->x + j + dx, lb->y + i + dy);
+          long long c = in.tap(lb, lb->x + j + dx, lb->y + i + dy);
           a += c * c;
           b += c;
         }
@@ -462,7 +475,6 @@ HD void lr_box(const FrameParams *fp, int plane, const LrBlock *lb, const uint8_
       A[i + 1][j + 1] = (int)a2;
       Bv[i + 1][j + 1] = (int)((b2 + (1LL << (SGRPROJ_RECIP_BITS - 1))) >> SGRPROJ_RECIP_BITS);
     }
-  int stride = fp->stride[plane];
   for (int i = 0; i < lb->h; i++) {
     int shift = 5;
     if (pass == 0 && (i & 1)) shift = 4;
@@ -476,7 +488,7 @@ HD void lr_box(const FrameParams *fp, int plane, const LrBlock *lb, const uint8_
           a += weight * A[i + dy + 1][j + dx + 1];
           b += weight * Bv[i + dy + 1][j + dx + 1];
         }
-      long long v = a * cdef[fp->offset[plane] + (lb->y + i) * stride + lb->x + j] + b;
+      long long v = a * in.own(lb->x + j, lb->y + i) + b;
       int sh = SGRPROJ_SGR_BITS + shift - SGRPROJ_RST_BITS;
       F[i * 4 + j] = (int)((v + (1LL << (sh - 1))) >> sh);
     }
@@ -484,33 +496,31 @@ HD void lr_box(const FrameParams *fp, int plane, const LrBlock *lb, const uint8_
 }
 
 // Self-guided projection (spec 7.17.2) of a block whose box-filter outputs
-// are flt0 / flt1, into sink(offset, value).
-template <class Sink>
-HD void lr_sgr_project(const FrameParams *fp, int plane, const LrBlock *lb, const uint8_t *cdef, const LrUnit *u,
-                       const int *flt0, const int *flt1, Sink &sink) {
+// are flt0 / flt1.
+template <class Src, class Sink>
+HD void lr_sgr_project(const LrBlock *lb, const Src &in, const LrUnit *u, const int *flt0, const int *flt1, Sink &sink) {
   int w0 = u->xqd[0], w1 = u->xqd[1];
   int w2 = (1 << SGRPROJ_PRJ_BITS) - w0 - w1;
   int r0 = T(Sgr_Params)[u->set][0], r1 = T(Sgr_Params)[u->set][2];
-  int stride = fp->stride[plane];
   for (int i = 0; i < lb->h; i++)
     for (int j = 0; j < lb->w; j++) {
-      int o = fp->offset[plane] + (lb->y + i) * stride + lb->x + j;
-      int uu = cdef[o] << SGRPROJ_RST_BITS;
+      int uu = in.own(lb->x + j, lb->y + i) << SGRPROJ_RST_BITS;
       int v = w1 * uu;
       v += r0 ? w0 * flt0[i * 4 + j] : w0 * uu;
       v += r1 ? w2 * flt1[i * 4 + j] : w2 * uu;
-      sink(o, clip3(0, 255, round2(v, SGRPROJ_RST_BITS + SGRPROJ_PRJ_BITS)));
+      sink(lb->x + j, lb->y + i, clip3(0, 255, round2(v, SGRPROJ_RST_BITS + SGRPROJ_PRJ_BITS)));
     }
 }
 
 // Self-guided filter (spec 7.17.2).
 HD void lr_sgr(const FrameParams *fp, int plane, const LrBlock *lb, const uint8_t *cdef, const uint8_t *dbk, uint8_t *out,
                const LrUnit *u) {
+  FrameSrc in{fp, plane, cdef, dbk};
   int flt0[16], flt1[16];
-  lr_box(fp, plane, lb, cdef, dbk, u->set, 0, flt0);
-  lr_box(fp, plane, lb, cdef, dbk, u->set, 1, flt1);
-  StoreSink sink{out};
-  lr_sgr_project(fp, plane, lb, cdef, u, flt0, flt1, sink);
+  lr_box(lb, in, u->set, 0, flt0);
+  lr_box(lb, in, u->set, 1, flt1);
+  StoreSink sink{fp, plane, out};
+  lr_sgr_project(lb, in, u, flt0, flt1, sink);
 }
 
 // Thread per (plane, 4x4 luma block): loop_restore_block( ) with the unit's

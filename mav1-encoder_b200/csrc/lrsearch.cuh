@@ -91,6 +91,62 @@ __device__ void unit_geom(const FrameParams *fp, int plane, int ur, int uc, Geom
     }
 }
 
+// A unit's samples staged in shared memory: the CDEF output, the deblocked
+// frame and the source over the unit plus 3 samples on every side (clamped to
+// the plane), which covers every tap the filters read for the unit's blocks
+// (get_source_sample moves a row at most to the block's own 3-row margin).
+// A unit spans at most 103 x 95 samples (the last unit row or column takes
+// the remainder, and unit rows are offset by 8 luma rows).
+constexpr int WP = 104, WH = 112;
+
+struct Win {
+  uint8_t cd[WH * WP], db[WH * WP], sr[WH * WP];
+  int x0, y0;
+};
+
+struct WinSrc {
+  const Win *w;
+  HD int tap(const LrBlock *lb, int x, int y) const {
+    x = imax(0, imin(lb->planeEndX, x));
+    y = imax(0, imin(lb->planeEndY, y));
+    const uint8_t *b = w->cd;
+    if (y < lb->stripeStart) {
+      y = imax(lb->stripeStart - 2, y);
+      b = w->db;
+    } else if (y > lb->stripeEnd) {
+      y = imin(lb->stripeEnd + 2, y);
+      b = w->db;
+    }
+    return b[(y - w->y0) * WP + (x - w->x0)];
+  }
+  HD int own(int x, int y) const { return w->cd[(y - w->y0) * WP + (x - w->x0)]; }
+  HD int src(int x, int y) const { return w->sr[(y - w->y0) * WP + (x - w->x0)]; }
+};
+
+// Copies the unit's window into shared memory (the whole CTA).
+__device__ void stage_window(const FrameParams *fp, const Geom &g, const uint8_t *cdef, const uint8_t *dbk,
+                             const uint8_t *src, Win &w) {
+  const int sub = g.plane > 0, bw = MI_SIZE >> sub;
+  const int endX = ((fp->frame_w + sub) >> sub) - 1, endY = ((fp->frame_h + sub) >> sub) - 1;
+  const int x0 = imax(0, ((g.c0 * MI_SIZE) >> sub) - 3), y0 = imax(0, ((g.r0 * MI_SIZE) >> sub) - 3);
+  const int x1 = imin(endX, ((g.c1 - 1) * MI_SIZE >> sub) + bw - 1 + 3);
+  const int y1 = imin(endY, ((g.r1 - 1) * MI_SIZE >> sub) + bw - 1 + 3);
+  const int nx = imin(WP, x1 - x0 + 1), ny = imin(WH, y1 - y0 + 1);
+  const int stride = fp->stride[g.plane], off = fp->offset[g.plane];
+  if (threadIdx.x == 0) {
+    w.x0 = x0;
+    w.y0 = y0;
+  }
+  for (int i = threadIdx.x; i < nx * ny; i += blockDim.x) {
+    int r = i / nx, c = i - r * nx;
+    int o = off + (y0 + r) * stride + x0 + c, k = r * WP + c;
+    w.cd[k] = cdef[o];
+    w.db[k] = dbk[o];
+    w.sr[k] = src[o];
+  }
+  __syncthreads();
+}
+
 // ---- double arithmetic exactly as the reference's C (no contraction) ---------
 __device__ __forceinline__ double dadd(double a, double b) { return __dadd_rn(a, b); }
 __device__ __forceinline__ double dsub(double a, double b) { return __dsub_rn(a, b); }
@@ -192,6 +248,7 @@ HD long long rd(const FrameParams *fp, long long sse, int bits) { return sse * 1
 
 // ---- CTA-wide helpers ------------------------------------------------------------------
 struct Shared {
+  Win win;
   double phi[2][ROWBUF][4];  // per sample of a block row: phi[0..nc) and the target
   double acc[12];
   double f[7], g[7];
@@ -213,37 +270,33 @@ __device__ long long cta_sum(long long v, Shared &sh) {
 }
 
 struct SseSink {
-  const uint8_t *src;
+  const Win *w;
   long long sse;
-  HD void operator()(int o, int v) {
-    int d = v - (int)src[o];
+  HD void operator()(int x, int y, int v) {
+    int d = v - (int)w->sr[(y - w->y0) * WP + (x - w->x0)];
     sse += d * d;
   }
 };
 
-// SSE of a unit filtered with u against the source (unit_sse): a thread per
-// 4x4 block of the unit.
-__device__ long long unit_sse(const FrameParams *fp, const Geom &g, const uint8_t *cdef, const uint8_t *dbk,
-                              const uint8_t *src, const LrUnit &u, Shared &sh) {
+// SSE of a unit filtered with u against the source (unit_sse), from the
+// staged window: a thread per 4x4 block of the unit.
+__device__ long long unit_sse(const FrameParams *fp, const Geom &g, const LrUnit &u, Shared &sh) {
   int nc = g.c1 - g.c0, nb = (g.r1 - g.r0) * nc;
-  SseSink sink{src, 0};
+  WinSrc in{&sh.win};
+  SseSink sink{&sh.win, 0};
   for (int b = threadIdx.x; b < nb; b += THREADS) {
     LrBlock lb;
     if (!lr_block_setup(fp, g.plane, g.r0 + b / nc, g.c0 + b % nc, &lb)) continue;
     if (u.type == RESTORE_WIENER) {
-      flt::lr_wiener_to(fp, g.plane, &lb, cdef, dbk, &u, sink);
+      flt::lr_wiener_to(&lb, in, &u, sink);
     } else if (u.type == RESTORE_SGRPROJ) {
       int flt0[16], flt1[16];
-      flt::lr_box(fp, g.plane, &lb, cdef, dbk, u.set, 0, flt0);
-      flt::lr_box(fp, g.plane, &lb, cdef, dbk, u.set, 1, flt1);
-      flt::lr_sgr_project(fp, g.plane, &lb, cdef, &u, flt0, flt1, sink);
+      flt::lr_box(&lb, in, u.set, 0, flt0);
+      flt::lr_box(&lb, in, u.set, 1, flt1);
+      flt::lr_sgr_project(&lb, in, &u, flt0, flt1, sink);
     } else {
-      int stride = fp->stride[g.plane];
       for (int i = 0; i < lb.h; i++)
-        for (int j = 0; j < lb.w; j++) {
-          int o = fp->offset[g.plane] + (lb.y + i) * stride + lb.x + j;
-          sink(o, cdef[o]);
-        }
+        for (int j = 0; j < lb.w; j++) sink(lb.x + j, lb.y + i, in.own(lb.x + j, lb.y + i));
     }
   }
   return cta_sum(sink.sse, sh);
@@ -259,11 +312,10 @@ HD LrUnit wiener_unit(const int w[2][3]) {
 
 // wiener_fit (lr_search.c:142-193): four alternating separable least-squares
 // solves, then the taps in coded units.
-__device__ void wiener_fit(const FrameParams *fp, const Geom &g, const uint8_t *cdef, const uint8_t *dbk,
-                           const uint8_t *src, Shared &sh, int out[2][3]) {
+__device__ void wiener_fit(const FrameParams *fp, const Geom &g, Shared &sh, int out[2][3]) {
   const int plane = g.plane, first = plane ? 1 : 0, nc = 3 - first, nacc = nc * nc + nc;
   const int sub = plane > 0, bwf = MI_SIZE >> sub;
-  const int stride = fp->stride[plane];
+  const WinSrc in{&sh.win};
   if (threadIdx.x < 7) {
     sh.f[threadIdx.x] = threadIdx.x == 3 ? 1.0 : 0.0;
     sh.g[threadIdx.x] = threadIdx.x == 3 ? 1.0 : 0.0;
@@ -295,14 +347,14 @@ __device__ void wiener_fit(const FrameParams *fp, const Geom &g, const uint8_t *
         for (int kk = 0; kk < 7; kk++) {
           double s = 0.0;
           for (int t = 0; t < 7; t++) {
-            int sv = vertical ? lr_src(fp, plane, &lb, cdef, dbk, lb.x + j + t - 3, lb.y + i + kk - 3)
-                              : lr_src(fp, plane, &lb, cdef, dbk, lb.x + j + kk - 3, lb.y + i + t - 3);
+            int sv = vertical ? in.tap(&lb, lb.x + j + t - 3, lb.y + i + kk - 3)
+                              : in.tap(&lb, lb.x + j + kk - 3, lb.y + i + t - 3);
             s = dadd(s, dmul(vertical ? sh.g[t] : sh.f[t], (double)sv));
           }
           Z[kk] = s;
         }
         for (int kk = first; kk < 3; kk++) sh.phi[buf][k][kk - first] = dsub(dadd(Z[kk], Z[6 - kk]), dmul(2.0, Z[3]));
-        sh.phi[buf][k][3] = dsub((double)src[fp->offset[plane] + (lb.y + i) * stride + lb.x + j], Z[3]);
+        sh.phi[buf][k][3] = dsub((double)in.src(lb.x + j, lb.y + i), Z[3]);
       }
       __syncthreads();
       if (threadIdx.x < nacc) {
@@ -351,22 +403,21 @@ __device__ void wiener_fit(const FrameParams *fp, const Geom &g, const uint8_t *
 // sgr_fit (lr_search.c:196-240): least-squares projection weights of set
 // `set`. The sums are integer-valued and exact in int64; the closing double
 // arithmetic follows the reference's operations.
-__device__ void sgr_fit(const FrameParams *fp, const Geom &g, const uint8_t *cdef, const uint8_t *dbk,
-                        const uint8_t *src, int set, Shared &sh, int xqd[2]) {
+__device__ void sgr_fit(const FrameParams *fp, const Geom &g, int set, Shared &sh, int xqd[2]) {
   const int r0 = T(Sgr_Params)[set][0], r1 = T(Sgr_Params)[set][2];
-  const int ncols = g.c1 - g.c0, nb = (g.r1 - g.r0) * ncols, stride = fp->stride[g.plane];
+  const int ncols = g.c1 - g.c0, nb = (g.r1 - g.r0) * ncols;
+  const WinSrc in{&sh.win};
   long long h00 = 0, h01 = 0, h11 = 0, c0 = 0, c1 = 0;
   for (int b = threadIdx.x; b < nb; b += THREADS) {
     LrBlock lb;
     if (!lr_block_setup(fp, g.plane, g.r0 + b / ncols, g.c0 + b % ncols, &lb)) continue;
     int flt0[16], flt1[16];
-    flt::lr_box(fp, g.plane, &lb, cdef, dbk, set, 0, flt0);
-    flt::lr_box(fp, g.plane, &lb, cdef, dbk, set, 1, flt1);
+    flt::lr_box(&lb, in, set, 0, flt0);
+    flt::lr_box(&lb, in, set, 1, flt1);
     for (int i = 0; i < lb.h; i++)
       for (int j = 0; j < lb.w; j++) {
-        int o = fp->offset[g.plane] + (lb.y + i) * stride + lb.x + j;
-        long long u = (long long)cdef[o] << SGRPROJ_RST_BITS;
-        long long s = ((long long)src[o] << SGRPROJ_RST_BITS) - u;
+        long long u = (long long)in.own(lb.x + j, lb.y + i) << SGRPROJ_RST_BITS;
+        long long s = ((long long)in.src(lb.x + j, lb.y + i) << SGRPROJ_RST_BITS) - u;
         long long f0 = r0 ? flt0[i * 4 + j] - u : 0, f1 = r1 ? flt1[i * 4 + j] - u : 0;
         h00 += f0 * f0;
         h01 += f0 * f1;
@@ -416,16 +467,17 @@ __global__ void __launch_bounds__(THREADS) k_lr_fit(const FrameParams *fp, const
   if (threadIdx.x == 0) unit_geom(fp, plane, u / fp->lr_unit_cols[plane], u % fp->lr_unit_cols[plane], &sh.geom);
   __syncthreads();
   const Geom g = sh.geom;
+  stage_window(fp, g, cdef, dbk, src, sh.win);
   Fit &F = fits[gu];
   LrUnit none = {};
   none.type = RESTORE_NONE;
-  long long sseNone = unit_sse(fp, g, cdef, dbk, src, none, sh);
+  long long sseNone = unit_sse(fp, g, none, sh);
   int w[2][3];
-  wiener_fit(fp, g, cdef, dbk, src, sh, w);
+  wiener_fit(fp, g, sh, w);
   // the fitted filter and its single-tap neighbours, in the refinement's order
   int n = 0;
   LrUnit base = wiener_unit(w);
-  long long sseW = unit_sse(fp, g, cdef, dbk, src, base, sh);
+  long long sseW = unit_sse(fp, g, base, sh);
   if (threadIdx.x == 0) {
     taps_of(base, F.taps[n]);
     F.sse[n] = sseW;
@@ -437,7 +489,7 @@ __global__ void __launch_bounds__(THREADS) k_lr_fit(const FrameParams *fp, const
         LrUnit t = base;
         t.wiener[pass][j] += d;
         if (t.wiener[pass][j] < T(Wiener_Taps_Min)[j] || t.wiener[pass][j] > T(Wiener_Taps_Max)[j]) continue;
-        long long sse = unit_sse(fp, g, cdef, dbk, src, t, sh);
+        long long sse = unit_sse(fp, g, t, sh);
         if (threadIdx.x == 0) {
           taps_of(t, F.taps[n]);
           F.sse[n] = sse;
@@ -446,13 +498,13 @@ __global__ void __launch_bounds__(THREADS) k_lr_fit(const FrameParams *fp, const
       }
   for (int set = 0; set < 16; set++) {
     int xqd[2];
-    sgr_fit(fp, g, cdef, dbk, src, set, sh, xqd);
+    sgr_fit(fp, g, set, sh, xqd);
     LrUnit s = {};
     s.type = RESTORE_SGRPROJ;
     s.set = set;
     s.xqd[0] = xqd[0];
     s.xqd[1] = xqd[1];
-    long long sse = unit_sse(fp, g, cdef, dbk, src, s, sh);
+    long long sse = unit_sse(fp, g, s, sh);
     if (threadIdx.x == 0) {
       F.xqd[set][0] = xqd[0];
       F.xqd[set][1] = xqd[1];
@@ -468,9 +520,10 @@ __global__ void __launch_bounds__(THREADS) k_lr_fit(const FrameParams *fp, const
 }
 
 // SSE of Wiener candidate t: the first pass's value when it has one, else
-// computed by the whole CTA (every thread calls this with the same t).
+// computed by the whole CTA from the unit's window, staged at the first such
+// candidate of the unit (every thread calls this with the same t).
 __device__ long long wiener_sse(const FrameParams *fp, const Fit &F, const Geom &g, const uint8_t *cdef,
-                                const uint8_t *dbk, const uint8_t *src, const LrUnit &t, Shared &sh) {
+                                const uint8_t *dbk, const uint8_t *src, const LrUnit &t, Shared &sh, bool &staged) {
   int tt[6];
   taps_of(t, tt);
   for (int i = 0; i < F.n; i++) {
@@ -478,7 +531,11 @@ __device__ long long wiener_sse(const FrameParams *fp, const Fit &F, const Geom 
     for (int k = 0; k < 6; k++) eq = eq && F.taps[i][k] == tt[k];
     if (eq) return F.sse[i];
   }
-  return unit_sse(fp, g, cdef, dbk, src, t, sh);
+  if (!staged) {
+    stage_window(fp, g, cdef, dbk, src, sh.win);
+    staged = true;
+  }
+  return unit_sse(fp, g, t, sh);
 }
 
 // Second pass: one CTA per plane, the units in order (lr_select's loop,
@@ -509,6 +566,7 @@ __global__ void __launch_bounds__(THREADS) k_lr_select(FrameParams *fp, const ui
     long long bestCost = rd(fp, F.sse_none, 1);
     int tw[2][3], tx[2];
     LrUnit w = wiener_unit(F.w);
+    bool staged = false;
     memcpy(tw, refW, sizeof tw);
     memcpy(tx, refX, sizeof tx);
     long long wc = rd(fp, F.sse[0], 2 + unit_bits(plane, w, tw, tx));
@@ -520,7 +578,7 @@ __global__ void __launch_bounds__(THREADS) k_lr_select(FrameParams *fp, const ui
           if (t.wiener[pass][j] < T(Wiener_Taps_Min)[j] || t.wiener[pass][j] > T(Wiener_Taps_Max)[j]) continue;
           memcpy(tw, refW, sizeof tw);
           memcpy(tx, refX, sizeof tx);
-          long long tc = rd(fp, wiener_sse(fp, F, g, cdef, dbk, src, t, sh), 2 + unit_bits(plane, t, tw, tx));
+          long long tc = rd(fp, wiener_sse(fp, F, g, cdef, dbk, src, t, sh, staged), 2 + unit_bits(plane, t, tw, tx));
           if (tc < wc) {
             wc = tc;
             w = t;

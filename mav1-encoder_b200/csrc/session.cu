@@ -426,6 +426,8 @@ extern "C" int mav1cu_session_create(int width, int height, int max_cdef_presets
     s->resident_recon = imax(1, sms * imin(1, imax(1, per)));
   }
   cudaFuncSetAttribute(ana::k_analyze_level, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ANA_SMEM(16));
+  cudaFuncSetAttribute(lrs::k_lr_fit, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(lrs::Shared));
+  cudaFuncSetAttribute(lrs::k_lr_select, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(lrs::Shared));
   *out = s;
   return MAV1CU_OK;
 }
