@@ -671,7 +671,10 @@ def main():
                 "gpu_launches": int(r["launches"]), "clocks": r["clocks"],
                 "roofline": roofline(r["kern"], peaks)}
         if not args.no_batch:
-            line["batch"] = batch_bench(args)
+            try:
+                line["batch"] = batch_bench(args)
+            except Exception as ex:  # reported in the line; the clip's numbers stand on their own
+                line["batch"] = {"error": f"{type(ex).__name__}: {ex}"}
         if not args.no_cpu_baseline:
             fps, wall, ideal = cpu_reference(args.cpu_sample)
             line["cpu_baseline"] = {"value": round(fps, 3), "unit": "fps", "cores": cores, "kind": "reference",

@@ -70,7 +70,7 @@ struct Ctx {
   int32_t *coefs;
   const int32_t *mats;
   const int32_t *mats_t;  // the same matrices transposed
-  int *status;          // [0] error code, [1] abort
+  int *status;          // [0] error (1 ready-queue wait, 2 successor list, 3 chroma-edge wait), [1] abort
   const int *blk_at;    // per 4x4 luma unit of the frame: index of the block covering it
   int *done;            // per block index: 1 once its luma samples are written; then the same for chroma
   // the intra blocks' ready queue: unfinished luma dependencies per block,
@@ -798,7 +798,7 @@ __device__ void wait_units(const Ctx &c, const Smem &sm, int group, const int *r
     while (!vdone[b]) {
       if (vstatus[1] || ++spins > c.spin_limit) {
         if (!vstatus[1]) {
-          atomicExch(c.status, 1);
+          atomicExch(c.status, 3);  // 3: a chroma-edge wait gave up
           atomicExch(c.status + 1, 1);
         }
         break;

@@ -74,6 +74,9 @@ struct mav1cu_session {
   // internal device state
   uint8_t *qp[2];          // 16 quarter-pel planes per reference
   uint8_t *dsrc, *dref[2]; // decimated planes
+  // planes of the references supplied by a stream for the next motion
+  // search (its per-picture cache); null: the search builds its own
+  const uint8_t *ext_qp[2], *ext_dref[2];
   uint8_t *ys, *uvs;       // edge-type marks per mi
   int32_t *mats_t;         // MATS with every matrix transposed (row passes read it along the output index)
   int mats_dirty;          // MATS changed since mats_t was derived
@@ -497,7 +500,13 @@ static int build_waves(mav1cu_session *s, int tile_w_sb) {
     s->wave_len[w] = (int)list.size() - s->wave_start[w];
   }
   s->wave_tile_w = tile_w_sb;
-  return check_cuda(s, cudaMemcpy(s->waves, list.data(), list.size() * sizeof(int), cudaMemcpyHostToDevice), "waves");
+  // in the session's stream order: a plain cudaMemcpy from pageable memory
+  // may return before the data lands, and the stream's kernels (non-blocking
+  // stream) would not wait for it; the async copy stages the list before it
+  // returns
+  return check_cuda(s, cudaMemcpyAsync(s->waves, list.data(), list.size() * sizeof(int), cudaMemcpyHostToDevice,
+                                       s->stream),
+                    "waves");
 }
 
 extern "C" int mav1cu_set_params(mav1cu_session *s, const mav1cu_frame_params *fp) {
@@ -525,37 +534,52 @@ static int need_params(mav1cu_session *s) {
 #define DP(s) ((const FrameParams *)(s)->buf[MAV1CU_BUF_PARAMS])
 #define U8(s, b) ((uint8_t *)(s)->buf[b])
 
+// The motion search's planes of one reference picture (padded layout) on
+// the session's stream: the 16 quarter-pel planes and, in the T_ME_DEC mode,
+// the decimated plane.
+static int build_ref_planes(mav1cu_session *s, const uint8_t *ref, uint8_t *qp, uint8_t *dref) {
+  const FrameParams &fp = s->fp;
+  dim3 qgrid((fp.frame_w + me::QP_TW - 1) / me::QP_TW, (fp.frame_h + me::QP_TH - 1) / me::QP_TH);
+  me::k_qpel_planes<<<qgrid, me::QP_THREADS, 0, s->stream>>>(DP(s), ref, qp);
+  if (after_launch(s, "qpel planes")) return s->err;
+  if (fp.turbo & T_ME_DEC) {
+    int dw = (fp.frame_w + 3) >> 2, dh = (fp.frame_h + 3) >> 2;
+    me::k_dec_plane<<<dim3((dw + 127) / 128, dh), 128, 0, s->stream>>>(DP(s), ref, dref);
+    if (after_launch(s, "decimated reference")) return s->err;
+  }
+  return MAV1CU_OK;
+}
+
 extern "C" int mav1cu_motion_search(mav1cu_session *s) {
   if (need_params(s)) return s->err;
   const FrameParams &fp = s->fp;
   int nref = fp.golden ? 2 : 1;
   const uint8_t *refs[2] = {U8(s, MAV1CU_BUF_REF), U8(s, MAV1CU_BUF_GOLD)};
+  const uint8_t *qp[2] = {s->qp[0], s->qp[1]}, *dref[2] = {s->dref[0], s->dref[1]};
   if (fp.turbo & T_ME_HPEL) {
-    dim3 blk(128);
-    dim3 qgrid((fp.frame_w + me::QP_TW - 1) / me::QP_TW, (fp.frame_h + me::QP_TH - 1) / me::QP_TH);
     for (int r = 0; r < nref; r++) {
-      me::k_qpel_planes<<<qgrid, me::QP_THREADS, 0, s->stream>>>(DP(s), refs[r], s->qp[r]);
-      if (after_launch(s, "qpel planes")) return s->err;
+      if (s->ext_qp[r]) {  // supplied by the stream's plane cache, complete in stream order
+        qp[r] = s->ext_qp[r];
+        dref[r] = s->ext_dref[r];
+      } else if (build_ref_planes(s, refs[r], s->qp[r], s->dref[r])) {
+        return s->err;
+      }
     }
     if (fp.turbo & T_ME_DEC) {
       int dw = (fp.frame_w + 3) >> 2, dh = (fp.frame_h + 3) >> 2;
-      dim3 dg((dw + 127) / 128, dh);
-      me::k_dec_plane<<<dg, blk, 0, s->stream>>>(DP(s), U8(s, MAV1CU_BUF_SRC), s->dsrc);
+      me::k_dec_plane<<<dim3((dw + 127) / 128, dh), 128, 0, s->stream>>>(DP(s), U8(s, MAV1CU_BUF_SRC), s->dsrc);
       if (after_launch(s, "decimated source")) return s->err;
-      for (int r = 0; r < nref; r++) {
-        me::k_dec_plane<<<dg, blk, 0, s->stream>>>(DP(s), refs[r], s->dref[r]);
-        if (after_launch(s, "decimated reference")) return s->err;
-      }
     }
   }
+  for (int r = 0; r < 2; r++) s->ext_qp[r] = s->ext_dref[r] = nullptr;
   me::Frame f[2];
   for (int r = 0; r < 2; r++) {
     f[r].fp = DP(s);
     f[r].src = U8(s, MAV1CU_BUF_SRC);
     f[r].ref = refs[r];
-    f[r].qp = s->qp[r];
+    f[r].qp = qp[r];
     f[r].dsrc = s->dsrc;
-    f[r].dref = s->dref[r];
+    f[r].dref = dref[r];
     f[r].mv = (int32_t *)s->buf[r ? MAV1CU_BUF_MVGOLD : MAV1CU_BUF_MVFIELD];
     f[r].isGold = r;
   }
@@ -685,12 +709,17 @@ extern "C" int mav1cu_debug_recon_fault(mav1cu_session *s, int hold_block, int s
   return MAV1CU_OK;
 }
 
-extern "C" int mav1cu_frame_core(mav1cu_session *s) {
-  if (need_params(s)) return s->err;
-  if (!s->fp.frame_is_intra && mav1cu_motion_search(s)) return s->err;
+// The frame core after the motion search: analysis, edge types, recon.
+static int frame_core_after_me(mav1cu_session *s) {
   if (mav1cu_analyze(s)) return s->err;
   if (s->fp.enable_intra_edge_filter && mav1cu_edge_types(s)) return s->err;
   return mav1cu_recon(s);
+}
+
+extern "C" int mav1cu_frame_core(mav1cu_session *s) {
+  if (need_params(s)) return s->err;
+  if (!s->fp.frame_is_intra && mav1cu_motion_search(s)) return s->err;
+  return frame_core_after_me(s);
 }
 
 extern "C" int mav1cu_filter_info(mav1cu_session *s) {
@@ -913,7 +942,9 @@ extern "C" int mav1cu_synchronize(mav1cu_session *s) {
   if (check_cuda(s, cudaMemcpy(st, s->status, sizeof st, cudaMemcpyDeviceToHost), "status")) return s->err;
   if (st[0])
     return set_error(s, MAV1CU_ERR_DEVICE, "device status %d: %s", st[0],
-                     st[0] == 2 ? "a recon successor list overflowed" : "a recon dependency wait gave up");
+                     st[0] == 2   ? "a recon successor list overflowed"
+                     : st[0] == 3 ? "a recon chroma-edge dependency wait gave up"
+                                  : "a recon ready-queue wait gave up");
   return MAV1CU_OK;
 }
 
@@ -1020,7 +1051,48 @@ struct mav1cu_stream {
   std::vector<EventRef> readers[8];   // reference copies of the slot's picture since then
   size_t i420_bytes;
   int last_engine;
+  // Motion-search planes per reference picture (the quarter-pel and
+  // decimated planes depend on the picture alone): the engines' own plane
+  // buffers serve as PLANE_SETS entries, each tagged with the picture it
+  // holds. A reference frame's planes are built once, on its engine, right
+  // after its slots are written; later frames that reference the picture use
+  // them. Hazards are events: a user waits for `built`, a rebuild waits for
+  // every motion search that read the entry's previous picture.
+  struct PlaneSet {
+    uint8_t *qp, *dref;
+    int64_t pic = -1;               // picture held (-1: none)
+    int64_t used = 0;               // last use, for least-recently-used replacement
+    EventRef built;
+    std::vector<EventRef> readers;
+  } planes[2 * NUM_ENGINES];
+  int64_t slot_pic[8];              // picture in each reference slot (-1: none)
+  int64_t pic_seq, plane_clock;
 };
+
+// Entry holding picture `pic`, or -1.
+static int plane_find(mav1cu_stream *st, int64_t pic) {
+  for (int i = 0; i < 2 * NUM_ENGINES; i++)
+    if (pic >= 0 && st->planes[i].pic == pic) return i;
+  return -1;
+}
+
+// Builds the planes of picture `pic` (its samples in `ref`, padded layout)
+// into the least recently used entry other than `keep`, on engine s's
+// stream, after every reader of that entry's previous picture.
+static int plane_build(mav1cu_stream *st, mav1cu_session *s, const uint8_t *ref, int64_t pic, int keep) {
+  int v = -1;
+  for (int i = 0; i < 2 * NUM_ENGINES; i++)
+    if (i != keep && (v < 0 || st->planes[i].used < st->planes[v].used)) v = i;
+  auto &e = st->planes[v];
+  for (auto &r : e.readers) cudaStreamWaitEvent(s->stream, r->e, 0);
+  e.readers.clear();
+  if (build_ref_planes(s, ref, e.qp, e.dref)) return -1;
+  e.built = std::make_shared<Event>();
+  cudaEventRecord(e.built->e, s->stream);
+  e.pic = pic;
+  e.used = ++st->plane_clock;
+  return v;
+}
 
 extern "C" int mav1cu_stream_create(const mav1cu_config *cfg, mav1cu_stream **out, char *err, size_t errlen) {
   *out = NULL;
@@ -1036,6 +1108,11 @@ extern "C" int mav1cu_stream_create(const mav1cu_config *cfg, mav1cu_stream **ou
   }
   size_t fb = st->eng[0]->g.frame_bytes;
   st->i420_bytes = (size_t)n.c.width * n.c.height + 2 * (size_t)((n.c.width + 1) >> 1) * ((n.c.height + 1) >> 1);
+  for (int i = 0; i < 2 * NUM_ENGINES; i++) {
+    st->planes[i].qp = st->eng[i >> 1]->qp[i & 1];
+    st->planes[i].dref = st->eng[i >> 1]->dref[i & 1];
+  }
+  for (int k = 0; k < 8; k++) st->slot_pic[k] = -1;
   cudaError_t e = cudaSuccess;
   for (int k = 0; k < 8 && e == cudaSuccess; k++) {
     e = cudaMalloc(&st->slot[k], fb);
@@ -1072,6 +1149,10 @@ extern "C" void mav1cu_stream_destroy(mav1cu_stream *st) {
     st->readers[k].clear();
     if (st->slot[k]) cudaFree(st->slot[k]);
   }
+  for (auto &p : st->planes) {
+    p.built.reset();
+    p.readers.clear();
+  }
   for (int e = 0; e < NUM_ENGINES; e++) {
     for (int b = 0; b < 2; b++) {
       if (st->staging[e][b]) cudaFree(st->staging[e][b]);
@@ -1094,6 +1175,12 @@ extern "C" int mav1cu_stream_reconfigure(mav1cu_stream *st, const mav1cu_config 
   for (int k = 0; k < 8; k++) {
     st->written[k].reset();
     st->readers[k].clear();
+    st->slot_pic[k] = -1;
+  }
+  for (auto &p : st->planes) {
+    p.pic = -1;
+    p.built.reset();
+    p.readers.clear();
   }
   return MAV1CU_OK;
 }
@@ -1205,7 +1292,40 @@ extern "C" int mav1cu_stream_encode(mav1cu_stream *st, const mav1cu_frame_job *j
   FrameParams fp;
   int presets = 0;
   drv::frame_params(st->n, *job, &fp, &presets);
-  if (mav1cu_set_params(s, &fp) || mav1cu_frame_core(s)) return s->err;
+  if (mav1cu_set_params(s, &fp)) return s->err;
+  // the motion search's reference planes from the per-picture cache: a hit
+  // waits for the build, a miss builds them here from this frame's copy
+  int mePlanes = !fp.frame_is_intra && (fp.turbo & T_ME_HPEL), used[2] = {-1, -1};
+  if (mePlanes) {
+    int nref = fp.golden ? 2 : 1, refs[2] = {job->last_slot, job->arf_slot};
+    int64_t pic[2];
+    for (int r = 0; r < nref; r++) {
+      pic[r] = refs[r] >= 0 ? st->slot_pic[refs[r]] : -1;
+      used[r] = plane_find(st, pic[r]);
+    }
+    for (int r = 0; r < nref; r++) {
+      if (used[r] < 0) used[r] = plane_find(st, pic[r]);  // the other reference may have built it
+      if (used[r] >= 0) {
+        cudaStreamWaitEvent(s->stream, st->planes[used[r]].built->e, 0);
+        st->planes[used[r]].used = ++st->plane_clock;
+      } else {
+        // not cached (replaced, or a slot never written): a picture of its own
+        if (pic[r] < 0) pic[r] = ++st->pic_seq;
+        used[r] = plane_build(st, s, U8(s, r ? MAV1CU_BUF_GOLD : MAV1CU_BUF_REF), pic[r], used[1 - r]);
+        if (used[r] < 0) return s->err;
+      }
+      s->ext_qp[r] = st->planes[used[r]].qp;
+      s->ext_dref[r] = st->planes[used[r]].dref;
+    }
+  }
+  if (!fp.frame_is_intra && mav1cu_motion_search(s)) return s->err;
+  if (mePlanes) {
+    EventRef rd = std::make_shared<Event>();
+    cudaEventRecord(rd->e, s->stream);
+    for (int r = 0; r < 2; r++)
+      if (used[r] >= 0 && (r == 0 || used[1] != used[0])) st->planes[used[r]].readers.push_back(rd);
+  }
+  if (frame_core_after_me(s)) return s->err;
   // filter stage gating of run_frame_core (encoder.c:617-632)
   int nPresets = c.cdef ? 4 : 0, cdefOff = (job->leafopt & 4) != 0;
   int lfOn = fp.lf_level[0] || fp.lf_level[1] || fp.lf_level[2] || fp.lf_level[3];
@@ -1231,11 +1351,18 @@ extern "C" int mav1cu_stream_encode(mav1cu_stream *st, const mav1cu_frame_job *j
   if (rf) {
     out = std::make_shared<Event>();
     cudaEventRecord(out->e, s->stream);
+    int64_t pic = ++st->pic_seq;
+    int any = 0;
     for (int k = 0; k < 8; k++)
       if (((rf >> k) & 1) && slot_exists(st->n, k)) {
         st->written[k] = out;
         st->readers[k].clear();
+        st->slot_pic[k] = pic;
+        any = 1;
       }
+    // a new reference picture: its motion-search planes, once, from REC
+    // (the slots' copy source), for every later frame that references it
+    if (any && (fp.turbo & T_ME_HPEL) && plane_build(st, s, U8(s, MAV1CU_BUF_REC), pic, -1) < 0) return s->err;
   }
   return check_cuda(s, cudaGetLastError(), "stream encode");
 }

@@ -97,6 +97,7 @@ typedef struct Job {
   Mav1FrameStats st;
   double t0;
   int failed;
+  int xstatus;              /* the export header's status when it reported the failure (1 over capacity, 2 invalid blocks) */
   atomic_int state;         /* 0 free, 1 submitted, 2 coded */
 } Job;
 
@@ -474,7 +475,14 @@ static void write_ready(struct Mav1Encoder *e) {
     if (e->written == e->submitted || atomic_load(&j->state) != 2) break;
     if (j->failed && !e->err) {
       e->err = j->failed;
-      snprintf(e->msg, sizeof e->msg, "frame %d: device error %d", j->job.disp, j->failed);
+      /* what failed: the export's own checks, or a kernel's status word (the
+       * session's synchronize turns that into its message) */
+      const char *why = "";
+      if (j->xstatus == 1) why = "the export image's capacity was exceeded";
+      else if (j->xstatus == 2) why = "the export found blocks out of range";
+      else if (j->failed == MAV1CU_ERR_DEVICE && mav1cu_synchronize(j->sess) != MAV1CU_OK)
+        why = mav1cu_error_string(j->sess);
+      snprintf(e->msg, sizeof e->msg, "frame %d: device error %d%s%s", j->job.disp, j->failed, *why ? ": " : "", why);
       fprintf(stderr, "mav1 (cuda): %s\n", e->msg);
     }
     if (!e->tu_open) tu_open(e, j->job.is_key ? 0 : 1);
@@ -601,7 +609,10 @@ static void run_task(Task t) {
     pthread_mutex_unlock(&e->mu);
     const mav1cu_export_header *h = (const mav1cu_export_header *)j->img->image;
     if (j->failed || h->status != 0 || h->seq != (int32_t)j->seq) {
-      if (!j->failed) j->failed = h->status ? MAV1CU_ERR_DEVICE : MAV1CU_ERR_ARG;
+      if (!j->failed) {
+        j->failed = h->status ? MAV1CU_ERR_DEVICE : MAV1CU_ERR_ARG;
+        j->xstatus = h->status;
+      }
       frame_failed(j);
       return;
     }
