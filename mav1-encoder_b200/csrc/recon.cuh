@@ -46,7 +46,10 @@ namespace rec {
 #ifndef MAV1CU_INTER_THREADS
 #define MAV1CU_INTER_THREADS 128
 #endif
-constexpr int INTER_THREADS = MAV1CU_INTER_THREADS, INTRA_THREADS = 128;
+#ifndef MAV1CU_INTRA_THREADS
+#define MAV1CU_INTRA_THREADS 128
+#endif
+constexpr int INTER_THREADS = MAV1CU_INTER_THREADS, INTRA_THREADS = MAV1CU_INTRA_THREADS;
 #define FWD_SLOT_SIZE 4096
 HD int fwd_slot(int kind, int log2n) { return (kind * 5 + log2n - 2) * FWD_SLOT_SIZE; }
 
@@ -118,6 +121,7 @@ struct Smem {
   const uint8_t *srcp[3];
   int sstride[3];
   FrameParams fpc;           // the CTA's copy of the frame parameters
+  uint64_t qinv[3][2];       // per plane: the quantiser's reciprocals of dc_q and ac_q (tx::quant_inv)
   int cornerAR[3], cornerBL[3];  // BlockDecoded of those units
   int32_t fmat[3][FMAT_SMALL];  // forward matrices of lengths 4, 8, 16 per kind
   int32_t fmatT[3][FMAT_SMALL]; // the same transposed
@@ -523,7 +527,7 @@ __device__ __forceinline__ int code_tx(const Ctx &c, Smem &sm, const uint8_t *sr
   int single = numCands == 1 && !fp->tx_mode_select;
   int shifts = T(Transform_Row_Shift)[txSz] + 4, rect = iabs(lw - lh) == 1;
   int denom = tx::dq_denom(txSz);
-  uint64_t invDc = tx::quant_inv(dcQ), invAc = tx::quant_inv(acQ);
+  uint64_t invDc = sm.qinv[plane][0], invAc = sm.qinv[plane][1];  // derived once per CTA (load_shared)
   long long bestCost = -1;
   int bestType = DCT_DCT, bestEob = 0;
   int32_t *qsrc = sm.q;  // levels the final reconstruction uses
@@ -1315,6 +1319,11 @@ __device__ Ctx load_shared(const Ctx &c, Smem &sm) {
   for (int k = threadIdx.x; k < (int)(sizeof(FrameParams) / 4); k += RT) dst[k] = src[k];
   Ctx cs = c;
   cs.fp = &sm.fpc;
+  // the reciprocals are 64-bit divisions: once per CTA, not per transform block
+  if (threadIdx.x < 6) {
+    int p = threadIdx.x >> 1, q = (threadIdx.x & 1) ? c.fp->ac_q[p] : c.fp->dc_q[p];
+    sm.qinv[p][threadIdx.x & 1] = q > 0 ? tx::quant_inv(q) : 0;
+  }
   for (int kind = 0; kind < 3; kind++)
     for (int lg = 2; lg <= 4; lg++) {
       int n = 1 << (2 * lg), off = lg == 2 ? 0 : lg == 3 ? 16 : 80;

@@ -83,3 +83,40 @@ def test_dropin_full_tools_2160p_matches_golden(tmp_path):
     assert h(b"".join(p.tobytes() for r in recons for p in r)) == want["recon"]
     assert h(open(dump, "rb").read()) == want["dump"]
 
+
+
+@pytest.mark.skipif(not (oracle.available() and oracle.available(oracle.HYB_PATH)), reason="oracle not built")
+def test_dropin_throughput_1080p():
+    """What an unchanged mav1.h caller gets through the drop-in (the
+    reference's own serial driver with backend_cuda.c behind the vtable):
+    the benchmark clip's first 60 frames (1920x1080, --turbo -q 125 --keyint
+    60 --tiles 2), timed by wall clock, against the encoder API library on
+    the same frames. Every hook of the drop-in copies the encoder's full host
+    buffers to and from the device and synchronises, so it is far slower
+    than the API library; the printed figures show by how much. Both
+    bitstreams equal the reference CPU path's."""
+    import time
+
+    import mav1api
+    import mav1cu
+
+    spec, n = synthetic.CONFIGS["c1_1080p"], 60
+    flags = dict(q=125, turbo=1, keyint=60, tiles=2)
+    frames = list(synthetic.generate(spec, n))
+    pk_cpu, _ = oracle.encode(frames, oracle.cli_config(spec.width, spec.height, cpu=True, **flags))
+    cfg_hyb = oracle.cli_config(spec.width, spec.height, cpu=False, **flags)
+    oracle.encode(frames[:2], cfg_hyb, factory="cuda", path=oracle.HYB_PATH)  # warm-up
+    t0 = time.perf_counter()
+    pk_hyb, _ = oracle.encode(frames, cfg_hyb, factory="cuda", path=oracle.HYB_PATH)
+    t_hyb = time.perf_counter() - t0
+    packed = [np.frombuffer(synthetic.packed(f), np.uint8) for f in frames]
+    cfg_api = mav1cu.cli_config(spec.width, spec.height, **flags)
+    mav1api.encode(packed[:2], cfg_api, recon=False)  # warm-up
+    t0 = time.perf_counter()
+    pk_api, _ = mav1api.encode(packed, cfg_api, recon=True)
+    t_api = time.perf_counter() - t0
+    ivf = lambda pk: oracle.ivf_bytes(pk, spec.width, spec.height)
+    assert ivf(pk_hyb) == ivf(pk_cpu)
+    assert mav1api.ivf_bytes(pk_api, spec.width, spec.height) == ivf(pk_cpu)
+    print(f"\ndrop-in (reference driver + backend_cuda.c): {n / t_hyb:.1f} fps; "
+          f"encoder API library (libmav1.so), one encoder: {n / t_api:.1f} fps")
