@@ -318,7 +318,7 @@ def run_ours(args, rank, world):
     ms_seq, _ = timed(step_sequential, max(1, args.steps // 2), 1)
     per_step = sum(ms) / len(ms)
     per_seq = sum(ms_seq) / len(ms_seq)
-    kern = kernel_times(streams[0].session, S, frames_dev) if (rank == 0 and not args.no_roofline) else None
+    kern = kernel_times(frames_dev) if (rank == 0 and not args.no_roofline) else None
     for st in streams:
         st.close()
     del frames_dev, flush
@@ -400,67 +400,145 @@ def e2e_api(args, frames_host, world):
                 threads=int(os.environ.get("MAV1_CUDA_THREADS", os.cpu_count())))
 
 
-def kernel_times(sess, stream, frames_dev):
-    """Device times for the roofline, with CUDA events on the stream the
-    kernels are launched on.
+def stage_calls(sess, presets, intra):
+    """The backend's stages of one frame on an engine session, in order."""
+    calls = [] if intra else [("motion_search", sess.motion_search)]
+    return calls + [("analyze", sess.analyze), ("edge_types", sess.edge_types), ("recon", sess.recon),
+                    ("filter_info", sess.filter_info), ("filter", lambda: sess.filter(presets)),
+                    ("cdef_select", lambda: sess.cdef_select(4))]
 
-    dominant: the reconstruction stage of the clip's first key frame, which is
-    the dominant kernel k_recon_blocks (the intra block workers, 28% of the
-    clip's device time in the ncu launch list) plus four short set-up
-    launches.
-    A fresh stream codes the key frame, then the stage is re-run on the engine
-    session that holds the frame's analysis output (recon reproduces its
-    outputs from the same inputs). stage_ms: every stage of one ALTREF frame,
-    for reference."""
-    import torch
+
+def frame_stages(frames_dev, fn, kinds=("key", "arf")):
+    """Codes the clip's first key and ALTREF frames through a fresh stream,
+    and after each one calls fn(kind, engine session, stage list) while the
+    engine still holds that frame's inputs (a stage re-run reproduces its
+    outputs from them; the frame's reference slots were written already)."""
     import mav1cu
 
     cfg = mav1cu.cli_config(SPEC.width, SPEC.height, **FLAGS)
     jobs = mav1cu.plan(cfg, SPEC.frames)
-    key = jobs[0]
+    picks = {"key": jobs[0], "arf": next(j for j in jobs if j["kind"] == 1)}
     st = mav1cu.Stream(cfg)
-    st.encode(key, frames_dev[key["disp"]].data_ptr(), True)
-    st.synchronize()
-    es = st.engines[st.engine_of(key)]
-    ext = torch.cuda.ExternalStream(st.lib.mav1cu_get_stream(es.h))
-    ts = []
-    for i in range(8):
-        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
-        ev[0].record(ext)
-        es.recon()
-        ev[1].record(ext)
-        ev[1].synchronize()
-        if i >= 3:
-            ts.append(ev[0].elapsed_time(ev[1]))
-    es.synchronize()
-    key_recon_ms = statistics.median(ts)
-    st.close()
+    out = {}
+    try:
+        for kind in ("key", "arf"):
+            j = picks[kind]
+            st.encode(j, frames_dev[j["disp"]].data_ptr(), True)
+            st.synchronize()
+            if kind not in kinds:
+                continue
+            es = st.engines[st.engine_of(j)]
+            fp, presets = mav1cu.frame_params(cfg, j)
+            es.set_params(fp)
+            out[kind] = fn(kind, es, stage_calls(es, presets, kind == "key"))
+            es.synchronize()
+    finally:
+        st.close()
+    return out
 
-    # every stage of one ALTREF frame (inputs: whatever the session holds)
-    sess.set_stream(stream.cuda_stream)
-    arf = next(j for j in jobs if j["kind"] == 1)
-    fp, presets = mav1cu.frame_params(cfg, arf)
-    sess.set_params(fp)
-    stages = [("motion_search", sess.motion_search), ("analyze", sess.analyze), ("edge_types", sess.edge_types),
-              ("recon", sess.recon), ("filter_info", sess.filter_info), ("filter", lambda: sess.filter(presets)),
-              ("cdef_select", lambda: sess.cdef_select(4))]
-    res = {}
-    with torch.cuda.stream(stream):
-        for _ in range(3):
-            for name, fn in stages:
+
+def kernel_times(frames_dev):
+    """Device time of every stage of the clip's first key and ALTREF frames
+    (CUDA events on the engine's own stream, median of 5 after 2 warm-up
+    runs). The key frame's recon stage is the dominant kernel k_recon_blocks
+    (the intra block workers) plus four short set-up launches."""
+    import torch
+
+    def timeit(kind, es, calls):
+        ext = torch.cuda.ExternalStream(es.lib.mav1cu_get_stream(es.h))
+        res = {}
+        for _ in range(2):
+            for name, fn in calls:
                 fn()
-        stream.synchronize()
-        for name, fn in stages:
-            ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        es.synchronize()
+        for name, fn in calls:
             tt = []
             for _ in range(5):
-                ev[0].record(stream)
+                ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+                ev[0].record(ext)
                 fn()
-                ev[1].record(stream)
+                ev[1].record(ext)
                 ev[1].synchronize()
                 tt.append(ev[0].elapsed_time(ev[1]))
             res[name] = statistics.median(tt)
-    return {"key_recon_ms": key_recon_ms, "arf_stage_ms": res}
+        return res
+
+    return frame_stages(frames_dev, timeit)
+
+
+def work_counts():
+    """The counting build's work units of every stage of the same two frames
+    (one run of each stage between a reset and a read), and the device's
+    measured integer-operation peak. Runs in its own process (the counting
+    library's kernels and counters)."""
+    import ctypes
+    import torch
+    import mav1cu
+
+    mav1cu._lib = lib_ = mav1cu.load_count_library()
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+    frames_dev = torch.from_numpy(load_clip(SPEC)[:8]).cuda()
+
+    def count(kind, es, calls):
+        res = {}
+        for name, fn in calls:
+            es.synchronize()
+            lib_.mav1cu_work_reset()
+            fn()
+            es.synchronize()
+            res[name] = {k: v for k, v in mav1cu.work_read(lib_).items() if v}
+        return res
+
+    out = frame_stages(frames_dev, count)
+    peak = ctypes.c_double()
+    if lib_.mav1cu_work_int_peak(ctypes.byref(peak)) != 0:
+        raise RuntimeError("mav1cu_work_int_peak failed")
+    out["int_peak_ops_s"] = peak.value
+    return out
+
+
+# Integer operations per counted unit (include/mav1cu_count.h): a SAD byte
+# pair is an absolute difference and an add; a 4x4 SATD unit 16 differences,
+# the two Hadamard passes (64 adds), 16 absolute values and 16 adds; an
+# inter-predicted sample 8 + 8 multiply-accumulates; an intra-predicted
+# sample about 4 (DC none, SMOOTH 4 multiply-adds); a CfL SSE term a
+# multiply, round, clip, difference and square-add; a multiply-accumulate 2;
+# a quantised coefficient about 8 (scale, round, 64-bit reciprocal multiply,
+# shifts, sign); inverse-transform and loop-restoration counts are operations
+# and taps of 2; a CDEF tap about 6 (difference, constrain, weight, add).
+WORK_OPS = {"me_sad": 2, "me_dec_sad": 2, "me_satd": 112, "qpel_taps": 2, "ana_satd": 112, "ana_inter_px": 32,
+            "ana_intra_px": 4, "ana_cfl": 6, "rec_inter_px": 32, "rec_intra_px": 4, "fwd_mac": 2, "quant": 8,
+            "inv_ops": 1, "lf_taps": 2, "cdef_taps": 6, "lr_taps": 2}
+
+
+def run_work_counts():
+    """work_counts() in a child process (the counting library must not share
+    a process with the product library); None if it fails."""
+    try:
+        r = subprocess.run([sys.executable, os.path.abspath(__file__), "--work-counts"], capture_output=True, text=True,
+                           timeout=600)
+        return json.loads(r.stdout.strip().splitlines()[-1]) if r.returncode == 0 else None
+    except Exception:
+        return None
+
+
+def int_roofline(times, counts):
+    """Counted integer operations of every stage of the key and ALTREF
+    frames over the stage's device time, against the measured peak."""
+    peak = counts.get("int_peak_ops_s")
+    out = []
+    for kind in ("key", "arf"):
+        for stage, ms in times.get(kind, {}).items():
+            units = counts.get(kind, {}).get(stage, {})
+            ops = sum(WORK_OPS[k] * v for k, v in units.items())
+            ent = {"frame": kind, "stage": stage, "ms": round(ms, 4), "int_ops": ops, "units": units}
+            if ops and ms > 0:
+                ent["int_ops_per_s"] = round(ops / (ms * 1e-3) / 1e12, 4)
+                ent["frac_of_int_peak"] = round(ops / (ms * 1e-3) / peak, 5) if peak else None
+            out.append(ent)
+    return {"unit": "Tops/s", "peak_int_ops_per_s": round(peak / 1e12, 2) if peak else None,
+            "peak_source": "measured (mav1cu_work_int_peak: multiply-add, xor, add chains on every SM)",
+            "stages": out}
 
 
 # Bytes the key-frame reconstruction must move at 1080p, each once: source
@@ -487,20 +565,23 @@ STAGE_NCU = {
 }
 
 
-def roofline(kern, peaks):
+def roofline(kern, peaks, counts=None):
     """Roofline of the dominant kernel (k_recon_blocks) through its stage on
     the key frame: algorithmic bytes over the measured stage time, against the
     measured HBM copy bandwidth. The kernel is a dependency chain (latency
-    bound), so the fraction is small by nature; `stages` gives every stage's
-    live time on an ALTREF frame with its main kernel's integer-pipe
-    utilisation from the committed ncu captures."""
+    bound), so the fraction is small by nature; `stages_altref_frame` gives
+    every stage's live time on an ALTREF frame with its main kernel's
+    integer-pipe utilisation from the committed ncu captures, and `int_ops`
+    the counted integer operations of every stage of the key and ALTREF
+    frames against the measured integer peak (counts: work_counts())."""
     if not kern:
         return None
-    t = kern["key_recon_ms"] * 1e-3
+    key_recon_ms = kern["key"]["recon"]
+    t = key_recon_ms * 1e-3
     peak = peaks.get("hbm_gbs", 6650.0)
     achieved = KEY_RECON_BYTES / t / 1e9
     stages = []
-    for name, ms in kern["arf_stage_ms"].items():
+    for name, ms in kern["arf"].items():
         ent = {"stage": name, "ms": round(ms, 4)}
         if name in STAGE_NCU:
             k, alu, issue, src = STAGE_NCU[name]
@@ -508,8 +589,9 @@ def roofline(kern, peaks):
         stages.append(ent)
     return {"bound": "hbm", "kernel": "k_recon_blocks (key-frame recon stage)", "achieved": round(achieved, 2),
             "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 6), "traffic": KEY_RECON_DRAM_BYTES,
-            "algorithmic_bytes": KEY_RECON_BYTES, "ms_per_launch": round(kern["key_recon_ms"], 3),
+            "algorithmic_bytes": KEY_RECON_BYTES, "ms_per_launch": round(key_recon_ms, 3),
             "stages_altref_frame": stages,
+            "int_ops": int_roofline(kern, counts) if counts else None,
             "peak_source": "MEASURED_PEAKS.json" if "hbm_gbs" in peaks else "fallback"}
 
 
@@ -588,12 +670,18 @@ def main():
                          "full-tool configuration")
     ap.add_argument("--full4k-passes", type=int, default=1)
     ap.add_argument("--serving-sessions", type=int, default=400)
+    ap.add_argument("--work-counts", action="store_true",
+                    help="print the counting build's per-stage work units of the clip's first key and ALTREF frames "
+                         "and the measured integer peak (JSON), then exit")
     ap.add_argument("--profile-frames", type=int, default=0,
                     help="code the clip's first N planned frames once and exit (a short run for ncu)")
     ap.add_argument("--profile-export", action="store_true", help="with --profile-frames: export every frame")
     ap.add_argument("--profile-lr", action="store_true",
                     help="with --profile-frames: a 640x360 clip with every tool on (loop restoration)")
     args = ap.parse_args()
+    if args.work_counts:
+        print(json.dumps(work_counts()))
+        return
     if args.profile_frames:
         profile_run(args.profile_frames, export=args.profile_export, lr=args.profile_lr)
         return
@@ -669,7 +757,7 @@ def main():
                 "schedule": {"gop_parallel_streams": r["gops"], "frame_engines_per_stream": 2,
                              "fps_one_stream": round(frames / (r["ms_seq"] * 1e-3), 2)},
                 "gpu_launches": int(r["launches"]), "clocks": r["clocks"],
-                "roofline": roofline(r["kern"], peaks)}
+                "roofline": roofline(r["kern"], peaks, run_work_counts() if r["kern"] else None)}
         if not args.no_batch:
             try:
                 line["batch"] = batch_bench(args)

@@ -55,19 +55,32 @@ def stale(target, deps):
     return any(os.path.getmtime(d) > t for d in deps)
 
 
-def build(force=False, verbose=False, extra=()):
+def build(force=False, verbose=False, extra=(), out=LIB):
     deps = sources()
-    if not force and not stale(LIB, deps):
-        return LIB
+    if not force and not stale(out, deps):
+        return out
     cmd = [NVCC, *NVCC_FLAGS, *extra, "-I", os.path.join(ROOT, "include"), "-I", CSRC,
-           os.path.join(CSRC, "session.cu"), os.path.join(CSRC, "edge_noalloc.cu"), "-o", LIB + ".tmp"]
+           os.path.join(CSRC, "session.cu"), os.path.join(CSRC, "edge_noalloc.cu"), "-o", out + ".tmp"]
     if verbose:
         print(" ".join(cmd), file=sys.stderr)
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError("nvcc failed:\n" + r.stdout + r.stderr)
-    os.replace(LIB + ".tmp", LIB)
-    return LIB
+    os.replace(out + ".tmp", out)
+    return out
+
+
+COUNT_LIB = os.path.join(HERE, "libmav1cu_count.so")
+
+
+def build_count(force=False, verbose=False):
+    """libmav1cu_count.so: the same kernels with their work counters compiled
+    in (-DMAV1CU_COUNT, include/mav1cu_count.h), for the per-stage integer
+    operation counts of the benchmark; never on the coding path."""
+    deps = sources() + [os.path.join(ROOT, "include", "mav1cu_count.h")]
+    if not force and not stale(COUNT_LIB, deps):
+        return COUNT_LIB
+    return build(force=True, verbose=verbose, extra=("-DMAV1CU_COUNT",), out=COUNT_LIB)
 
 
 def build_api(force=False, verbose=False):
@@ -115,6 +128,7 @@ def build_cli(verbose=False):
 
 def build_all(force=False, verbose=False):
     build(force=force, verbose=verbose)
+    build_count(force=force, verbose=verbose)
     return build_api(force=force, verbose=verbose)
 
 

@@ -114,6 +114,8 @@ __device__ int inter_plane_satd(const FrameParams *fp, const uint8_t *src, const
     for (int r = 0; r < 4; r++)
       for (int c = 0; c < 4; c++) d[r * 4 + c] = (int)sp[(uy + r) * stride + ux + c] - d[r * 4 + c];
     s += pred::satd4x4(d);
+    WORK(W_ANA_SATD, 1);
+    WORK(W_ANA_INTER_PX, 16);
   }
   return gsum(s, g) * usub;
 }
@@ -152,6 +154,8 @@ __device__ void inter3(const FrameParams *fp, const uint8_t *src, const uint8_t 
       l0 += pred::satd4x4(d0);
       l1 += pred::satd4x4(d1);
       l2 += pred::satd4x4(d2);
+      WORK(W_ANA_SATD, 3);
+      WORK(W_ANA_INTER_PX, 32);
     }
     a0 += (long long)l0 * usub;
     a1 += (long long)l1 * usub;
@@ -216,6 +220,8 @@ __device__ int intra_mode_satd(const FrameParams *fp, const uint8_t *plane, int 
         d[r * 4 + c] = (int)sp[(uy + r) * stride + ux + c] - pv;
       }
     s += pred::satd4x4(d);
+    WORK(W_ANA_SATD, 1);
+    WORK(W_ANA_INTRA_PX, 16);
   }
   return gsum(s, g);
 }
@@ -236,6 +242,7 @@ __device__ int cfl_plane_satd(const FrameParams *fp, const uint8_t *src, int p, 
   int avg = round2(gsum(sum, g), clw + clh);
   int sse[33];
   for (int al = 0; al < 33; al++) sse[al] = 0;
+  if (g.rank == 0) WORK(W_ANA_CFL, n * 33);
   for (int k = g.rank; k < n; k += g.size) {
     int i = k / cw, j = k % cw;
     int v = pred::cfl_luma(luma, ls, cx, cy, maxLumaW, maxLumaH, i, j) - avg;
@@ -264,6 +271,8 @@ __device__ int cfl_plane_satd(const FrameParams *fp, const uint8_t *src, int p, 
         d[r * 4 + c] = (int)sp[(uy + r) * stride + ux + c] - pred::cfl_pixel(dc, bestA, v, avg);
       }
     s += pred::satd4x4(d);
+    WORK(W_ANA_SATD, 1);
+    WORK(W_ANA_INTRA_PX, 16);
   }
   return gsum(s, g);
 }

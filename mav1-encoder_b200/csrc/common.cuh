@@ -24,6 +24,32 @@ typedef mav1cu_block_info BlockInfo;
 typedef mav1cu_sb_info SbInfo;
 typedef mav1cu_lr_unit LrUnit;
 
+// ---- work counters (the counting build, -DMAV1CU_COUNT) ---------------------
+// Algorithmic work units per category, added by the kernels where the work
+// is done and read through include/mav1cu_count.h. The product library is
+// built without them (WORK compiles to nothing). Units:
+//   W_ME_SAD / W_ME_DSAD   full-pel SAD byte pairs, full resolution / decimated planes
+//   W_ME_SATD, W_ANA_SATD  4x4 Hadamard SATD units (motion search / analysis)
+//   W_QPEL_TAPS            filter taps of the quarter-pel planes (horizontal + vertical)
+//   W_ANA_INTER_PX, W_REC_INTER_PX  inter-predicted samples (8-tap horizontal + vertical each)
+//   W_ANA_INTRA_PX, W_REC_INTRA_PX  intra-predicted samples
+//   W_ANA_CFL              (sample, alpha) SSE terms of the CfL alpha searches
+//   W_REC_FWD_MAC          multiply-accumulates of the forward transform's two matrix passes
+//   W_REC_QUANT            quantised coefficients
+//   W_REC_INV_OPS          inverse transform operations (per 1D N-point pass, 3 log2 N per point)
+//   W_LF_TAPS, W_CDEF_TAPS, W_LR_TAPS  filter taps applied by deblocking, CDEF, loop restoration
+enum {
+  W_ME_SAD, W_ME_DSAD, W_ME_SATD, W_QPEL_TAPS, W_ANA_SATD, W_ANA_INTER_PX, W_ANA_INTRA_PX, W_ANA_CFL,
+  W_REC_INTER_PX, W_REC_INTRA_PX, W_REC_FWD_MAC, W_REC_QUANT, W_REC_INV_OPS, W_LF_TAPS, W_CDEF_TAPS, W_LR_TAPS,
+  W_COUNT
+};
+#if defined(MAV1CU_COUNT) && defined(__CUDACC__)
+static __device__ unsigned long long d_work[W_COUNT];
+#define WORK(cat, n) atomicAdd(&d_work[cat], (unsigned long long)(n))
+#else
+#define WORK(cat, n) ((void)0)
+#endif
+
 // ---- AV1 enumerations (specification section 6.10) -------------------------
 enum { INTRA_FRAME = 0, LAST_FRAME = 1, GOLDEN_FRAME = 4, ALTREF_FRAME = 7 };
 enum {

@@ -157,6 +157,7 @@ __global__ void k_deblock(const FrameParams *fp, uint8_t *rec, const uint8_t *mi
   int baseSize = pass == 0 ? imin(T(Tx_Width)[prevTxSz], T(Tx_Width)[txSz]) : imin(T(Tx_Height)[prevTxSz], T(Tx_Height)[txSz]);
   int filterSize = plane == 0 ? imin(16, baseSize) : imin(8, baseSize);
   int sx = xP + dy * i, sy = yP + dx * i;
+  WORK(W_LF_TAPS, filterSize == 4 ? 4 : (plane != 0 ? 6 : (filterSize == 8 ? 8 : 16)));  // the line's filter length
   lf_sample(base + sy * stride + sx, pass == 0 ? 1 : stride, plane, lvl, fp->lf_sharpness, filterSize);
 }
 
@@ -205,6 +206,7 @@ __global__ void __launch_bounds__(64) k_cdef(const FrameParams *fp, const uint8_
   int r = (blockIdx.x / bc) * 2, c = (blockIdx.x % bc) * 2;
   int tid = threadIdx.x;
   int skip = (info[r * fp->mi_cols + c] >> 5) & 1;
+  if (tid == 0 && !skip) WORK(W_CDEF_TAPS, 64 * 8);  // direction search: 64 samples into 8 projections
   if (!skip) {
     for (int k = tid; k < 8 * 15; k += 64) partial[k / 15][k % 15] = 0;
     __syncthreads();
@@ -255,6 +257,7 @@ __global__ void __launch_bounds__(64) k_cdef(const FrameParams *fp, const uint8_
     int priStr = fp->cdef_y_pri[idx], secStr = fp->cdef_y_sec[idx];
     int uvPri = fp->cdef_uv_pri[idx], uvSec = fp->cdef_uv_sec[idx];
     int copyOnly = skip || (priStr == 0 && secStr == 0 && uvPri == 0 && uvSec == 0);
+    if (tid == 0 && !copyOnly) WORK(W_CDEF_TAPS, (64 + 32) * 12);  // 12 taps per filtered sample
     // luma sample tid; chroma samples tid < 32 (16 per plane)
     {
       int i = tid >> 3, j = tid & 7, stride = fp->stride[0];
@@ -536,6 +539,7 @@ __global__ void k_lr_apply(const FrameParams *fp, const uint8_t *cdef, const uin
   LrUnit u;
   if (fp->lr_type[plane] == RESTORE_NONE) u.type = RESTORE_NONE;
   else u = units[fp->lr_unit_off[plane] + lb.unitRow * fp->lr_unit_cols[plane] + lb.unitCol];
+  WORK(W_LR_TAPS, lb.w * lb.h * (u.type == RESTORE_WIENER ? 14 : u.type == RESTORE_SGRPROJ ? 34 : 0));
   if (u.type == RESTORE_WIENER) {
     lr_wiener(fp, plane, &lb, cdef, dbk, out, &u);
   } else if (u.type == RESTORE_SGRPROJ) {

@@ -72,6 +72,8 @@ __global__ void __launch_bounds__(QP_THREADS) k_qpel_planes(const FrameParams *f
     }
   }
   __syncthreads();
+  // taps: the horizontal pass over the window (4 phases), the vertical pass per output of 16 planes
+  if (tid == 0) WORK(W_QPEL_TAPS, (QP_TH + 7) * QP_TW * 4 * 8 + imin(QP_TH, H - y0) * imin(QP_TW, W - x0) * 16 * 8);
   const int ty = tid >> 5, xx = (tid & 31) * 4, y = y0 + ty, x = x0 + xx;
   if (y >= H || x >= W) return;
   const size_t n = (size_t)W * H, o = (size_t)y * W + x;
@@ -324,6 +326,7 @@ __device__ void subpel_costs(const Frame &f, const Node &m, const int *cr, const
   int st = hp && (fp->turbo & T_ME_USUB) && m.w >= 32 ? 2 : 1;
   int nus = (nu + st - 1) / st;
   if (g.rank < ncand) cost[g.rank] = 0;
+  if (g.rank == 0) WORK(W_ME_SATD, ncand * nus);
   g.sync();
   for (int p = g.rank; p < ncand * nus; p += g.size) {
     int c = p / nus, u = (p % nus) * st;
@@ -371,6 +374,10 @@ __global__ void __launch_bounds__(128) k_me_level(Frame f0, Frame f1, int level,
   int by = 0, bx = 0;
   for (int stage = 0; stage < m.stages; stage++) {
     if (stage > 0) refine_stage(fp, &m, by, bx, stage);
+    if (grp.rank == 0) {  // byte pairs of the stage's candidates (full_cost)
+      int dec = (fp->turbo & T_ME_DEC) && m.step >= ME_COARSE_STEP, rs = (fp->turbo & T_ME_RSUB) && m.step == 1 ? 2 : 1;
+      WORK(dec ? W_ME_DSAD : W_ME_SAD, (long long)m.count * (dec ? (m.w >> 2) * (m.w >> 2) : (m.w / rs) * m.w));
+    }
     unsigned long long best = ~0ull;
     for (int k = grp.rank; k < m.count; k += grp.size) {
       int dy, dx;

@@ -386,6 +386,10 @@ __device__ __forceinline__ void inverse_2d_fixed(Smem &sm, const int32_t *q, int
 template <bool SMALL_INLINE>
 __device__ __forceinline__ void inverse_2d(Smem &sm, const int32_t *q, int txSz, int txType, int dcQ, int acQ,
                                            uint8_t *rec = nullptr, int rs = 0, int x = 0, int y = 0) {
+  if (threadIdx.x == 0) {  // h rows of w points, then w columns of h points: 3 log2 N operations per point
+    int lw = T(Tx_Width_Log2)[txSz], lh = T(Tx_Height_Log2)[txSz];
+    WORK(W_REC_INV_OPS, 3 * (1 << (lw + lh)) * (lw + lh));
+  }
   if (SMALL_INLINE) {
     int rsh = T(Transform_Row_Shift)[txSz];
     switch (txSz) {
@@ -541,6 +545,10 @@ __device__ __forceinline__ int code_tx(const Ctx &c, Smem &sm, const uint8_t *sr
     }
     __syncthreads();
     const int32_t *Mh = fwd_matrix_t(c, sm, tx::row_kind(t), lw), *Mv = fwd_matrix(c, sm, tx::col_kind(t), lh);
+    if (tid == 0) {  // row pass h x tw outputs of w terms, column pass th x tw outputs of h terms
+      WORK(W_REC_FWD_MAC, h * tw * w + th * tw * h);
+      WORK(W_REC_QUANT, th * tw);
+    }
     switch (lw) {
       case 2: fwd_rows<2>(sm, Mh, h); break;
       case 3: fwd_rows<3>(sm, Mh, h); break;
@@ -1024,6 +1032,7 @@ __device__ long long code_plane(const Ctx &c, Smem &sm, int plane, int txSz) {
         int tw = 1 << a.log2W, th = 1 << a.log2H;
         int dcv = a.mode == DC_PRED ? pred::intra_dc(a, above, left) : 0;
         uint8_t *d = px + startY * rs + startX;
+        if (threadIdx.x == 0) WORK(W_REC_INTRA_PX, tw * th);
         for (int k = threadIdx.x; k < tw * th; k += RT) {
           int i = k >> a.log2W, j = k & (tw - 1);
           d[i * rs + j] = (uint8_t)(a.mode == DC_PRED ? dcv : pred::intra_pixel(a, st, above, left, i, j));
@@ -1090,6 +1099,7 @@ __device__ long long code_plane(const Ctx &c, Smem &sm, int plane, int txSz) {
 __device__ void predict_block(Smem &sm, const pred::Inter &ip, int lw, int h, int mode, uint8_t *d, int ds) {
   int w = 1 << lw, W = w + 7, H = h + 7;
   uint8_t *win = (uint8_t *)sm.tmp;
+  if (threadIdx.x == 0) WORK(W_REC_INTER_PX, w * h);
   int16_t *hs = (int16_t *)sm.resid;
   for (int k = threadIdx.x; k < W * H; k += RT) {
     int R = k / W, C = k - R * W;

@@ -1366,3 +1366,81 @@ extern "C" int mav1cu_stream_encode(mav1cu_stream *st, const mav1cu_frame_job *j
   }
   return check_cuda(s, cudaGetLastError(), "stream encode");
 }
+
+// ---- the counting build (-DMAV1CU_COUNT, libmav1cu_count.so) ----------------------
+#ifdef MAV1CU_COUNT
+#include "mav1cu_count.h"
+
+extern "C" int mav1cu_work_read(uint64_t *out, int n) {
+  if (!out || n < W_COUNT) return MAV1CU_ERR_ARG;
+  unsigned long long v[W_COUNT];
+  if (cudaDeviceSynchronize() != cudaSuccess || cudaMemcpyFromSymbol(v, d_work, sizeof v) != cudaSuccess)
+    return MAV1CU_ERR_CUDA;
+  for (int i = 0; i < W_COUNT; i++) out[i] = v[i];
+  return W_COUNT;
+}
+
+extern "C" int mav1cu_work_reset(void) {
+  unsigned long long z[W_COUNT] = {};
+  if (cudaDeviceSynchronize() != cudaSuccess || cudaMemcpyToSymbol(d_work, z, sizeof z) != cudaSuccess)
+    return MAV1CU_ERR_CUDA;
+  return cudaDeviceSynchronize() == cudaSuccess ? MAV1CU_OK : MAV1CU_ERR_CUDA;
+}
+
+namespace {
+// Independent 32-bit integer chains per thread: per element and iteration a
+// multiply-add (the FMA pipe) and an exclusive-or plus an add (the ALU
+// pipe), 4 operations, none of which the compiler can merge.
+constexpr int PEAK_CHAINS = 8;
+__global__ void __launch_bounds__(256) k_int_peak(unsigned *out, int iters, unsigned seed) {
+  unsigned a[PEAK_CHAINS], b[PEAK_CHAINS];
+  for (int k = 0; k < PEAK_CHAINS; k++) {
+    a[k] = threadIdx.x * (k + 1) + seed;
+    b[k] = blockIdx.x ^ (seed * (k + 7));
+  }
+  for (int i = 0; i < iters; i++) {
+#pragma unroll
+    for (int k = 0; k < PEAK_CHAINS; k++) {
+      a[k] = a[k] * 2654435761u + b[k];
+      b[k] = (b[k] ^ a[k]) + 0x9e3779b9u;
+    }
+  }
+  unsigned s = 0;
+  for (int k = 0; k < PEAK_CHAINS; k++) s += a[k] ^ b[k];
+  if (s == seed) out[0] = s;  // keeps the chains live; practically never true
+}
+}  // namespace
+
+extern "C" int mav1cu_work_int_peak(double *ops_per_s) {
+  if (!ops_per_s) return MAV1CU_ERR_ARG;
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  unsigned *out = nullptr;
+  cudaStream_t st = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (cudaMalloc(&out, sizeof(unsigned)) != cudaSuccess) return MAV1CU_ERR_NOMEM;
+  cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  const int iters = 4096, ctas = sms * 8, threads = 256;
+  float best = 0;
+  for (int r = 0; r < 4; r++) {
+    cudaEventRecord(e0, st);
+    k_int_peak<<<ctas, threads, 0, st>>>(out, iters, 12345u + r);
+    cudaEventRecord(e1, st);
+    cudaEventSynchronize(e1);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (r > 0 && (best == 0 || ms < best)) best = ms;
+  }
+  cudaError_t e = cudaGetLastError();
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaStreamDestroy(st);
+  cudaFree(out);
+  if (e != cudaSuccess || best <= 0) return MAV1CU_ERR_CUDA;
+  *ops_per_s = 4.0 * PEAK_CHAINS * (double)iters * ctas * threads / (best * 1e-3);
+  return MAV1CU_OK;
+}
+#endif

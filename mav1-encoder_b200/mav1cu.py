@@ -149,6 +149,34 @@ def load_library(path=LIB_PATH):
     return lib
 
 
+COUNT_LIB_PATH = os.path.join(HERE, "libmav1cu_count.so")
+# the counting build's categories (include/mav1cu_count.h), in counter order
+WORK_NAMES = ["me_sad", "me_dec_sad", "me_satd", "qpel_taps", "ana_satd", "ana_inter_px", "ana_intra_px", "ana_cfl",
+              "rec_inter_px", "rec_intra_px", "fwd_mac", "quant", "inv_ops", "lf_taps", "cdef_taps", "lr_taps"]
+
+
+def load_count_library(path=COUNT_LIB_PATH):
+    """libmav1cu_count.so (every mav1cu entry point plus the work counters);
+    raises if it is missing."""
+    lib_ = load_library(path)
+    lib_.mav1cu_work_read.argtypes = [ctypes.c_void_p, ctypes.c_int]
+    lib_.mav1cu_work_read.restype = ctypes.c_int
+    lib_.mav1cu_work_reset.argtypes = []
+    lib_.mav1cu_work_reset.restype = ctypes.c_int
+    lib_.mav1cu_work_int_peak.argtypes = [ctypes.POINTER(ctypes.c_double)]
+    lib_.mav1cu_work_int_peak.restype = ctypes.c_int
+    return lib_
+
+
+def work_read(lib_):
+    """The counters of the counting build as {category: units}."""
+    v = np.zeros(len(WORK_NAMES), np.uint64)
+    rc = lib_.mav1cu_work_read(v.ctypes.data, len(WORK_NAMES))
+    if rc != len(WORK_NAMES):
+        raise Mav1cuError(f"mav1cu_work_read: {rc}")
+    return dict(zip(WORK_NAMES, (int(x) for x in v)))
+
+
 _lib = None
 
 
