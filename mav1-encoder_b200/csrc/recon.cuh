@@ -73,7 +73,7 @@ struct Ctx {
   int32_t *coefs;
   const int32_t *mats;
   const int32_t *mats_t;  // the same matrices transposed
-  int *status;          // [0] error (1 ready-queue wait, 2 successor list, 3 chroma-edge wait), [1] abort
+  int *status;          // [0] error (1 ready-queue wait, 2 successor list, 3 chroma-edge wait, 4 bulk copy), [1] abort
   const int *blk_at;    // per 4x4 luma unit of the frame: index of the block covering it
   int *done;            // per block index: 1 once its luma samples are written; then the same for chroma
   // the intra blocks' ready queue: unfinished luma dependencies per block,
@@ -123,16 +123,23 @@ struct Smem {
   FrameParams fpc;           // the CTA's copy of the frame parameters
   uint64_t qinv[3][2];       // per plane: the quantiser's reciprocals of dc_q and ac_q (tx::quant_inv)
   int cornerAR[3], cornerBL[3];  // BlockDecoded of those units
-  int32_t fmat[3][FMAT_SMALL];  // forward matrices of lengths 4, 8, 16 per kind
-  int32_t fmatT[3][FMAT_SMALL]; // the same transposed
   // What only one of the two kernels uses. k_recon_inter launches with the
-  // shared memory up to the end of pred0 (SMEM_INTER), k_recon_blocks with
-  // the whole struct, so neither holds the other's part on its SMs.
+  // shared memory up to the end of its part (SMEM_INTER), k_recon_blocks
+  // with the whole struct, so neither holds the other's part on its SMs.
   union {
     struct {  // inter blocks
       int16_t pred0[64 * 64];  // first compound prediction (intermediate precision)
+      // the superblock's source (luma 64 x 64, then the two 32 x 32 chroma
+      // planes), bulk-copied in once per CTA
+      __align__(16) uint8_t srcSB[64 * 64 + 2 * 32 * 32];
+      // the block plane being coded: prediction, then reconstruction, then
+      // written back to the frame
+      __align__(16) uint8_t recT[64 * 64];
+      __align__(8) unsigned long long bar;  // completion of the source copies
     };
     struct {  // intra blocks
+      int32_t fmat[3][FMAT_SMALL];   // forward matrices of lengths 4, 8, 16 per kind
+      int32_t fmatT[3][FMAT_SMALL];  // the same transposed
       int cbits;               // the block's corner bits (Ctx::corners)
       int succN;               // its successor count and list, copied while staging
       int succ[MAX_SUCC];
@@ -148,7 +155,7 @@ struct Smem {
     };
   };
 };
-constexpr size_t SMEM_INTER = offsetof(Smem, pred0) + sizeof(int16_t) * 64 * 64;
+constexpr size_t SMEM_INTER = offsetof(Smem, bar) + sizeof(unsigned long long);
 constexpr size_t SMEM_INTRA = sizeof(Smem);
 
 // Sums / maxima over the CTA. A one-warp CTA reduces by shuffles alone; the
@@ -408,15 +415,18 @@ __device__ __forceinline__ void inverse_2d(Smem &sm, const int32_t *q, int txSz,
   inverse_2d_large(sm, q, txSz, txType, dcQ, acQ, rec, rs, x, y);
 }
 
-// Forward matrix of a kind and length: lengths 4..16 from the CTA's shared
-// copy, 32 and 64 from the table in global memory; fwd_matrix_t gives the
-// transpose (the row pass reads it along the output index, so the lanes of
-// a warp read consecutive words).
+// Forward matrix of a kind and length: for the intra workers lengths 4..16
+// from the CTA's shared copy, otherwise (and for the inter kernel, whose
+// shared memory holds the superblock's source instead) from the table in
+// global memory; fwd_matrix_t gives the transpose (the row pass reads it
+// along the output index, so the lanes of a warp read consecutive words).
+template <bool INTER>
 __device__ __forceinline__ const int32_t *fwd_matrix(const Ctx &c, const Smem &sm, int kind, int lg) {
-  return lg <= 4 ? sm.fmat[kind] + (lg == 2 ? 0 : lg == 3 ? 16 : 80) : c.mats + fwd_slot(kind, lg);
+  return !INTER && lg <= 4 ? sm.fmat[kind] + (lg == 2 ? 0 : lg == 3 ? 16 : 80) : c.mats + fwd_slot(kind, lg);
 }
+template <bool INTER>
 __device__ __forceinline__ const int32_t *fwd_matrix_t(const Ctx &c, const Smem &sm, int kind, int lg) {
-  return lg <= 4 ? sm.fmatT[kind] + (lg == 2 ? 0 : lg == 3 ? 16 : 80) : c.mats_t + fwd_slot(kind, lg);
+  return !INTER && lg <= 4 ? sm.fmatT[kind] + (lg == 2 ? 0 : lg == 3 ? 16 : 80) : c.mats_t + fwd_slot(kind, lg);
 }
 
 // The transpose of every forward matrix (slot k: kind k / 5, length 4 << k % 5).
@@ -544,7 +554,7 @@ __device__ __forceinline__ int code_tx(const Ctx &c, Smem &sm, const uint8_t *sr
       sm.resid[i * 64 + j] = (int)src[(y + yy) * stride + x + xx] - (int)rec[(y + yy) * rs + x + xx];
     }
     __syncthreads();
-    const int32_t *Mh = fwd_matrix_t(c, sm, tx::row_kind(t), lw), *Mv = fwd_matrix(c, sm, tx::col_kind(t), lh);
+    const int32_t *Mh = fwd_matrix_t<INTER>(c, sm, tx::row_kind(t), lw), *Mv = fwd_matrix<INTER>(c, sm, tx::col_kind(t), lh);
     if (tid == 0) {  // row pass h x tw outputs of w terms, column pass th x tw outputs of h terms
       WORK(W_REC_FWD_MAC, h * tw * w + th * tw * h);
       WORK(W_REC_QUANT, th * tw);
@@ -1128,6 +1138,97 @@ __device__ void predict_block(Smem &sm, const pred::Inter &ip, int lw, int h, in
 }
 
 
+// ---- bulk copies (the TMA engine's cp.async.bulk) into shared memory ------------------
+__device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+// One row copy global -> shared, completing on the mbarrier: both addresses
+// 16-byte aligned, bytes a multiple of 16 (checked by the caller's layout).
+__device__ __forceinline__ void bulk_row(void *dst, const void *src, unsigned bytes, unsigned long long *bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+
+// Waits (bounded) for phase `parity` of the mbarrier to complete; false if
+// it did not within `limit` polls.
+__device__ __forceinline__ bool bar_wait(unsigned long long *bar, unsigned parity, int limit) {
+  for (int i = 0; i < limit; i++) {
+    unsigned done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+// The superblock's source (luma 64 rows of 64 bytes, two chroma planes of
+// 32 rows of 32 bytes) into sm.srcSB: one bulk copy per row, a thread each,
+// all completing on sm.bar. Rows are 16-byte aligned in the padded frame
+// layout (luma stride sb_cols * 64, chroma sb_cols * 32, superblock columns
+// at multiples of 64 / 32 bytes, plane offsets multiples of 64). On a wait
+// past the limit the error and abort words are set (status 4) and the copies
+// are waited for again before the CTA goes on, so none lands after it.
+__device__ void stage_sb_source(const Ctx &c, Smem &sm, int sb) {
+  static_assert(INTER_THREADS == 128, "one thread per source row");
+  const FrameParams *fp = c.fp;
+  int sbr = sb / fp->sb_cols, sbc = sb % fp->sb_cols, t = threadIdx.x;
+  if (t == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&sm.bar)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(&sm.bar)),
+                 "r"(64 * 64 + 2 * 32 * 32)
+                 : "memory");
+  }
+  __syncthreads();
+  if (t < 64) {
+    bulk_row(sm.srcSB + t * 64, c.src + fp->offset[0] + (size_t)(sbr * 64 + t) * fp->stride[0] + sbc * 64, 64, &sm.bar);
+  } else {
+    int p = 1 + ((t - 64) >> 5), r = (t - 64) & 31;
+    bulk_row(sm.srcSB + 64 * 64 + (p - 1) * 32 * 32 + r * 32,
+             c.src + fp->offset[p] + (size_t)(sbr * 32 + r) * fp->stride[p] + sbc * 32, 32, &sm.bar);
+  }
+  if (!bar_wait(&sm.bar, 0, c.spin_limit)) {
+    if (t == 0) {
+      atomicExch(c.status, 4);
+      atomicExch(c.status + 1, 1);
+    }
+    bar_wait(&sm.bar, 0, c.spin_limit);
+  }
+}
+
+// The inter block's plane p: views of the staged source (absolute plane
+// coordinates into sm.srcSB) and of sm.recT (the block's own w x h samples).
+__device__ __forceinline__ void inter_views(const Ctx &c, Smem &sm, int p) {
+  const BlockInfo &b = sm.blk;
+  int sub = p > 0, S = sub ? 32 : 64;
+  int sbx = (sm.c0 * 4) >> sub, sby = (sm.r0 * 4) >> sub;
+  const uint8_t *tile = sm.srcSB + (sub ? 64 * 64 + (p - 1) * 32 * 32 : 0);
+  int w = block_w(b.bsize) >> sub, x0 = (b.mi_col >> sub) * 4, y0 = (b.mi_row >> sub) * 4;
+  sm.srcp[p] = tile - ((ptrdiff_t)sby * S + sbx);
+  sm.sstride[p] = S;
+  sm.recp[p] = sm.recT - ((ptrdiff_t)y0 * w + x0);
+  sm.rstride[p] = w;
+}
+
+// Writes plane p of the inter block back from sm.recT to the frame (whole
+// words: block positions and widths are multiples of 4 samples).
+__device__ void unstage_inter(const Ctx &c, Smem &sm, int p) {
+  const FrameParams *fp = c.fp;
+  const BlockInfo &b = sm.blk;
+  int sub = p > 0, lw = floor_log2(block_w(b.bsize) >> sub) - 2, h = block_h(b.bsize) >> sub;
+  int x0 = (b.mi_col >> sub) * 4, y0 = (b.mi_row >> sub) * 4, fs = fp->stride[p];
+  uint8_t *g = c.rec + fp->offset[p] + y0 * fs + x0;
+  for (int k = threadIdx.x; k < (h << lw); k += RT) {
+    int i = k >> lw, j = k & ((1 << lw) - 1);
+    *(uint32_t *)(g + i * fs + 4 * j) = *(const uint32_t *)(sm.recT + (i << (lw + 2)) + 4 * j);
+  }
+  __syncthreads();
+}
+
 // Appends a block whose luma dependencies are complete to the ready queue.
 __device__ __forceinline__ void push_ready(const Ctx &c, int blk) {
   int t = atomicAdd(c.qtail, 1);
@@ -1160,21 +1261,17 @@ __device__ void recon_block(const Ctx &c, Smem &sm, BlockInfo *gb) {
     b.tx_depth = 0;
     b.interp_filter &= 0x30;
   }
-  if (INTER && threadIdx.x < 3) {
-    int p = threadIdx.x;
-    sm.recp[p] = c.rec + fp->offset[p];
-    sm.rstride[p] = fp->stride[p];
-    sm.srcp[p] = c.src + fp->offset[p];
-    sm.sstride[p] = fp->stride[p];
-  }
+  // inter blocks: the superblock's staged source and the block tile
+  // (one plane at a time, written back after it is coded)
+  if (INTER && threadIdx.x < 3) inter_views(c, sm, threadIdx.x);
   __syncthreads();
   if (!INTER) stage_begin(c, sm);
   int tid = threadIdx.x;
   if (INTER && fp->switchable_interp && !comp) {
     int w = block_w(bs), h = block_h(bs);
-    int x0 = MiCol * 4, y0 = MiRow * 4, stride = fp->stride[0], rs = sm.rstride[0];
+    int x0 = MiCol * 4, y0 = MiRow * 4, stride = fp->stride[0], ss = sm.sstride[0], rs = sm.rstride[0];
     uint8_t *px = sm.recp[0] + y0 * rs + x0;
-    const uint8_t *sp = c.src + fp->offset[0] + y0 * stride + x0;
+    const uint8_t *sp = sm.srcp[0] + y0 * ss + x0;
     int vw = imin(w, fp->frame_w - x0), vh = imin(h, fp->frame_h - y0);
     long long best = -1;
     int bestPacked = 0;
@@ -1188,7 +1285,7 @@ __device__ void recon_block(const Ctx &c, Smem &sm, BlockInfo *gb) {
       for (int k = tid; k < w * h; k += RT) {
         int i = k / w, j = k % w;
         if (i < vh && j < vw) {
-          int d = (int)px[i * rs + j] - (int)sp[i * stride + j];
+          int d = (int)px[i * rs + j] - (int)sp[i * ss + j];
           sse += d * d;
         }
       }
@@ -1229,17 +1326,13 @@ __device__ void recon_block(const Ctx &c, Smem &sm, BlockInfo *gb) {
         predict_block(sm, p0, floor_log2(w), h, 0, d, rs);
       }
     }
-    if (fp->lossless) {
-      code_plane<INTER>(c, sm, plane, TX_4X4);
-      continue;
-    }
-    if (plane > 0) {
-      code_plane<INTER>(c, sm, plane, uv_tx_size(bs, 1, 1));
-      continue;
-    }
-    int maxDepth = (!INTER && fp->tx_mode_select) ? imin(MAX_TX_DEPTH, T(Max_Tx_Depth)[bs]) : 0;
+    int maxDepth = (!INTER && fp->tx_mode_select && !fp->lossless && plane == 0)
+                       ? imin(MAX_TX_DEPTH, T(Max_Tx_Depth)[bs])
+                       : 0;
     if (maxDepth == 0) {
-      code_plane<INTER>(c, sm, 0, T(Max_Tx_Size_Rect)[bs]);
+      code_plane<INTER>(c, sm, plane,
+                        fp->lossless ? TX_4X4 : plane > 0 ? uv_tx_size(bs, 1, 1) : T(Max_Tx_Size_Rect)[bs]);
+      if (INTER) unstage_inter(c, sm, plane);
       continue;
     }
     // tx_depth RD search: every depth from the same pixels (BlockDecoded
@@ -1321,8 +1414,10 @@ __global__ void __launch_bounds__(1024) k_block_order(const BlockInfo *blocks, c
   if (t == 1023) *total = part[1023];
 }
 
-// The CTA's shared copies of the frame parameters and of the forward
-// matrices of lengths 4..16; returns the context reading them.
+// The CTA's shared copies of the frame parameters, the quantiser's
+// reciprocals and (intra workers) the forward matrices of lengths 4..16;
+// returns the context reading them.
+template <bool INTER>
 __device__ Ctx load_shared(const Ctx &c, Smem &sm) {
   const int *src = (const int *)c.fp;
   int *dst = (int *)&sm.fpc;
@@ -1334,17 +1429,20 @@ __device__ Ctx load_shared(const Ctx &c, Smem &sm) {
     int p = threadIdx.x >> 1, q = (threadIdx.x & 1) ? c.fp->ac_q[p] : c.fp->dc_q[p];
     sm.qinv[p][threadIdx.x & 1] = q > 0 ? tx::quant_inv(q) : 0;
   }
-  for (int kind = 0; kind < 3; kind++)
-    for (int lg = 2; lg <= 4; lg++) {
-      int n = 1 << (2 * lg), off = lg == 2 ? 0 : lg == 3 ? 16 : 80;
-      for (int k = threadIdx.x; k < n; k += RT) {
-        sm.fmat[kind][off + k] = c.mats[fwd_slot(kind, lg) + k];
-        sm.fmatT[kind][off + k] = c.mats_t[fwd_slot(kind, lg) + k];
+  if (!INTER)  // the inter kernel's shared memory ends before the intra part
+    for (int kind = 0; kind < 3; kind++)
+      for (int lg = 2; lg <= 4; lg++) {
+        int n = 1 << (2 * lg), off = lg == 2 ? 0 : lg == 3 ? 16 : 80;
+        for (int k = threadIdx.x; k < n; k += RT) {
+          sm.fmat[kind][off + k] = c.mats[fwd_slot(kind, lg) + k];
+          sm.fmatT[kind][off + k] = c.mats_t[fwd_slot(kind, lg) + k];
+        }
       }
-    }
   __syncthreads();
   return cs;
 }
+
+
 
 // The inter blocks of the frame, one CTA per superblock (all at once: they
 // read reference pictures only), each published complete for the intra
@@ -1352,8 +1450,13 @@ __device__ Ctx load_shared(const Ctx &c, Smem &sm) {
 __global__ void __launch_bounds__(INTER_THREADS, 512 / INTER_THREADS) k_recon_inter(Ctx cg) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Smem &sm = *(Smem *)smem_raw;
-  const Ctx c = load_shared(cg, sm);
+  const Ctx c = load_shared<true>(cg, sm);
   int sb = blockIdx.x, n = imax(0, imin(c.sbs[sb].num_blocks, MAX_BLOCKS_PER_SB));
+  if (threadIdx.x == 0) {
+    sm.r0 = (sb / c.fp->sb_cols) * 16;
+    sm.c0 = (sb % c.fp->sb_cols) * 16;
+  }
+  stage_sb_source(c, sm, sb);
   for (int k = 0; k < n; k++) {
     int me = sb * MAX_BLOCKS_PER_SB + k;
     if (threadIdx.x == 0) sm.blk = c.blocks[me];
@@ -1460,7 +1563,7 @@ __global__ void __launch_bounds__(INTRA_THREADS, 1) k_recon_blocks(Ctx cg, Claim
   int total = *q.total;
   if (blockIdx.x >= imax(MIN_WORKERS, total / BLOCKS_PER_WORKER)) return;
   Smem &sm = *(Smem *)smem_raw;
-  const Ctx c = load_shared(cg, sm);
+  const Ctx c = load_shared<false>(cg, sm);
   const FrameParams *fp = c.fp;
   volatile int *vstatus = c.status;
   for (;;) {

@@ -944,6 +944,7 @@ extern "C" int mav1cu_synchronize(mav1cu_session *s) {
     return set_error(s, MAV1CU_ERR_DEVICE, "device status %d: %s", st[0],
                      st[0] == 2   ? "a recon successor list overflowed"
                      : st[0] == 3 ? "a recon chroma-edge dependency wait gave up"
+                     : st[0] == 4 ? "a recon source bulk-copy wait gave up"
                                   : "a recon ready-queue wait gave up");
   return MAV1CU_OK;
 }
