@@ -558,9 +558,9 @@ KEY_RECON_DRAM_BYTES = 19914752
 # and leaf frames): the ALU pipe's share of its peak and the issue slots
 # active, ranges over the captured launches.
 STAGE_NCU = {
-    "motion_search": ("k_me_level", "31-41", "27-47", "profiles/k_me_level_1080p_turbo_3frames.md"),
-    "analyze": ("k_analyze_level", "20-27", "28-37", "profiles/k_analyze_level_1080p_turbo_3frames.md"),
-    "recon": ("k_recon_inter", "18", "26", "profiles/k_recon_inter_1080p_turbo_3frames.md"),
+    "motion_search": ("k_me_level", "31-48", "27-55", "profiles/k_me_level_1080p_turbo_3frames.md"),
+    "analyze": ("k_analyze_level", "23-31", "33-42", "profiles/k_analyze_level_1080p_turbo_3frames.md"),
+    "recon": ("k_recon_inter", "22", "31-33", "profiles/k_recon_inter_1080p_turbo_3frames.md"),
     "filter": ("k_deblock, k_cdef", "49-59", "63-67", "profiles/k_deblock_1080p_turbo_3frames.md"),
 }
 

@@ -546,7 +546,14 @@ __device__ int depth_pruned(const FrameParams *fp, const int64_t *costs, int sbI
 // group: threads per candidate (ANA_THREADS, 32 or 16; ana_groups gives the
 // edge scratch areas the dynamic shared memory holds).
 __host__ __device__ constexpr int ana_groups(int group) { return group < 32 ? ANA_THREADS / group : ANA_THREADS / 32; }
-__global__ void __launch_bounds__(ANA_THREADS) k_analyze_level(Ctx c, int level, int slots, int group) {
+// At least 4 CTAs per SM (at most 128 registers a thread): the level's
+// candidates are latency-bound SATD and filter sums, and the extra resident
+// warps hide more of it (measured on the 1080p clip: key-frame analysis
+// 2.47 -> 1.74 ms at 168 -> 128 registers; 5 CTAs spill and lose again).
+#ifndef MAV1CU_ANA_MIN_CTAS
+#define MAV1CU_ANA_MIN_CTAS 4
+#endif
+__global__ void __launch_bounds__(ANA_THREADS, MAV1CU_ANA_MIN_CTAS) k_analyze_level(Ctx c, int level, int slots, int group) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   WarpMem *wmem = (WarpMem *)smem_raw;
   long long *red = (long long *)(wmem + ana_groups(group));

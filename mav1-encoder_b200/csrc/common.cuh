@@ -47,7 +47,7 @@ enum {
 static __device__ unsigned long long d_work[W_COUNT];
 #define WORK(cat, n) atomicAdd(&d_work[cat], (unsigned long long)(n))
 #else
-#define WORK(cat, n) ((void)0)
+#define WORK(cat, n) ((void)(n))  // discarded (the operands have no side effects)
 #endif
 
 // ---- AV1 enumerations (specification section 6.10) -------------------------

@@ -341,7 +341,13 @@ __device__ void subpel_costs(const Frame &f, const Node &m, const int *cr, const
 // One search level: with group 128 the CTA's four warps per node (the 64x64
 // level: few, large nodes), with 32 a warp per (node, reference), with 16
 // half a warp (the 8x8 level); blockIdx.y selects the reference.
-__global__ void __launch_bounds__(128) k_me_level(Frame f0, Frame f1, int level, int group) {
+// At least 5 CTAs per SM (at most 102 registers a thread): more resident
+// warps hide the L2 latency of the candidates' SAD rows (measured on the
+// 1080p clip: an ALTREF frame's search 0.46 -> 0.36 ms; 8 CTAs spill).
+#ifndef MAV1CU_ME_MIN_CTAS
+#define MAV1CU_ME_MIN_CTAS 5
+#endif
+__global__ void __launch_bounds__(128, MAV1CU_ME_MIN_CTAS) k_me_level(Frame f0, Frame f1, int level, int group) {
   __shared__ int s_cost[8][16];
   __shared__ int s_r[8][16], s_c[8][16];
   __shared__ unsigned long long s_best[4];
