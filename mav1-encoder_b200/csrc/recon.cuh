@@ -1542,7 +1542,10 @@ __global__ void __launch_bounds__(128) k_block_deps(Ctx c, const int *list, cons
 #ifndef MAV1CU_BLOCKS_PER_WORKER
 #define MAV1CU_BLOCKS_PER_WORKER 8
 #endif
-constexpr int BLOCKS_PER_WORKER = MAV1CU_BLOCKS_PER_WORKER, MIN_WORKERS = 8;
+#ifndef MAV1CU_MIN_WORKERS
+#define MAV1CU_MIN_WORKERS 8
+#endif
+constexpr int BLOCKS_PER_WORKER = MAV1CU_BLOCKS_PER_WORKER, MIN_WORKERS = MAV1CU_MIN_WORKERS;
 
 struct Claim {
   const int *list;
