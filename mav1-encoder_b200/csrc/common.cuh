@@ -27,7 +27,8 @@ typedef mav1cu_lr_unit LrUnit;
 // ---- work counters (the counting build, -DMAV1CU_COUNT) ---------------------
 // Algorithmic work units per category, added by the kernels where the work
 // is done and read through include/mav1cu_count.h. The product library is
-// built without them (WORK compiles to nothing). Units:
+// built without them (WORK discards its operands, which have no side
+// effects, so no code remains). Units:
 //   W_ME_SAD / W_ME_DSAD   full-pel SAD byte pairs, full resolution / decimated planes
 //   W_ME_SATD, W_ANA_SATD  4x4 Hadamard SATD units (motion search / analysis)
 //   W_QPEL_TAPS            filter taps of the quarter-pel planes (horizontal + vertical)

@@ -16,10 +16,13 @@
 //                the SSE of the fitted filter and of its single-tap
 //                neighbours (the candidates the refinement tries first), and
 //                per self-guided set the fit and its SSE;
+//   k_lr_spec    one CTA per unit: the Wiener refinement replayed under
+//                guessed running references, caching the SSE of every
+//                candidate it visits (SSEs do not depend on the references);
 //   k_lr_select  one CTA per plane, units in order: the rate comparisons of
 //                lr_select with the running references; a refinement
-//                candidate that was not computed in the first pass (after an
-//                accepted step) is evaluated on the spot by the whole CTA.
+//                candidate whose SSE neither pass cached is evaluated on the
+//                spot by the whole CTA.
 //
 // Bit-exactness. SSEs, the self-guided sums and the first Wiener iteration
 // are integer-valued (every partial sum is an integer below 2^53, so double
@@ -41,7 +44,7 @@ using flt::lr_block_setup;
 using flt::lr_src;
 
 constexpr int THREADS = 256;
-constexpr int CACHE = 16;       // candidate SSEs a unit keeps from the first pass
+constexpr int CACHE = 40;       // candidate SSEs a unit keeps from the first pass and the speculative pass
 constexpr int ROWBUF = 4 * 96;  // samples of one block row of a unit (4 rows of at most 95)
 
 // What the first pass leaves for the serial choice, per unit.
@@ -255,6 +258,13 @@ struct Shared {
   long long red[THREADS / 32];
   Geom geom;
   int stop;
+  // k_lr_spec: the unit's candidate cache (Fit::taps / sse / n), kept by thread 0
+  int ctaps[CACHE][6];
+  long long csse[CACHE];
+  int cn;
+  // k_lr_select: the unit's first-pass results, and a cache lookup's result
+  Fit fit;
+  int found;
 };
 
 // Sum of v over the CTA (every thread gets it).
@@ -522,15 +532,29 @@ __global__ void __launch_bounds__(THREADS) k_lr_fit(const FrameParams *fp, const
 // SSE of Wiener candidate t: the first pass's value when it has one, else
 // computed by the whole CTA from the unit's window, staged at the first such
 // candidate of the unit (every thread calls this with the same t).
+// Index of the cache entry holding taps tt (entries are distinct), or -1:
+// thread i compares entry i (the whole CTA).
+__device__ int cache_find(const int (*taps)[6], int n, const int *tt, Shared &sh) {
+  if (threadIdx.x == 0) sh.found = -1;
+  __syncthreads();
+  int i = threadIdx.x;
+  if (i < n) {
+    bool eq = true;
+    for (int k = 0; k < 6; k++) eq = eq && taps[i][k] == tt[k];
+    if (eq) sh.found = i;
+  }
+  __syncthreads();
+  int f = sh.found;
+  __syncthreads();
+  return f;
+}
+
 __device__ long long wiener_sse(const FrameParams *fp, const Fit &F, const Geom &g, const uint8_t *cdef,
                                 const uint8_t *dbk, const uint8_t *src, const LrUnit &t, Shared &sh, bool &staged) {
   int tt[6];
   taps_of(t, tt);
-  for (int i = 0; i < F.n; i++) {
-    bool eq = true;
-    for (int k = 0; k < 6; k++) eq = eq && F.taps[i][k] == tt[k];
-    if (eq) return F.sse[i];
-  }
+  int f = cache_find(F.taps, F.n, tt, sh);
+  if (f >= 0) return F.sse[f];
   if (!staged) {
     stage_window(fp, g, cdef, dbk, src, sh.win);
     staged = true;
@@ -541,6 +565,91 @@ __device__ long long wiener_sse(const FrameParams *fp, const Fit &F, const Geom 
 // Second pass: one CTA per plane, the units in order (lr_select's loop,
 // lr_search.c:276-355). Every thread runs the same scalar decisions; the SSE
 // of a candidate the first pass did not compute is evaluated by all of them.
+// Speculative refinement, one CTA per unit, after k_lr_fit: the Wiener
+// refinement of lr_select (lr_search.c:296-318) replayed for the unit under
+// guessed running references, computing and caching the SSE of every
+// candidate the cache does not hold yet. An SSE depends on the candidate
+// filter and the unit's samples only, never on the references, so a cached
+// value is exactly what the serial choice would compute; the references only
+// decide which candidates the refinement visits. The guesses: the default
+// references (exact for a plane's first unit) and the fitted filter of each
+// of the two previous units (the true reference is usually the refined
+// filter of a recent unit). k_lr_select then finds most of its candidates
+// here and computes only the rest on the spot.
+__device__ void spec_path(const FrameParams *fp, int plane, const Geom &g, const uint8_t *cdef, const uint8_t *dbk,
+                          const uint8_t *src, const int fitted[2][3], const int ref[2][3], Shared &sh, bool &staged) {
+  LrUnit w = wiener_unit(fitted);
+  int tw[2][3], tx[2] = {0, 0};
+  memcpy(tw, ref, sizeof tw);
+  long long wc = rd(fp, sh.csse[0], 2 + unit_bits(plane, w, tw, tx));
+  for (int pass = 0; pass < 2; pass++)
+    for (int j = plane ? 1 : 0; j < 3; j++)
+      for (int d = -1; d <= 1; d += 2) {
+        LrUnit t = w;
+        t.wiener[pass][j] += d;
+        if (t.wiener[pass][j] < T(Wiener_Taps_Min)[j] || t.wiener[pass][j] > T(Wiener_Taps_Max)[j]) continue;
+        int tt[6];
+        taps_of(t, tt);
+        int n = sh.cn;
+        int f = cache_find(sh.ctaps, n, tt, sh);
+        long long sse = f >= 0 ? sh.csse[f] : -1;
+        if (sse < 0) {
+          if (n >= CACHE) return;  // full: the serial choice computes the rest
+          if (!staged) {
+            stage_window(fp, g, cdef, dbk, src, sh.win);
+            staged = true;
+          }
+          sse = unit_sse(fp, g, t, sh);  // the whole CTA; every thread gets the sum
+          if (threadIdx.x == 0) {
+            for (int k = 0; k < 6; k++) sh.ctaps[n][k] = tt[k];
+            sh.csse[n] = sse;
+            sh.cn = n + 1;
+          }
+          __syncthreads();
+        }
+        memcpy(tw, ref, sizeof tw);
+        long long tc = rd(fp, sse, 2 + unit_bits(plane, t, tw, tx));
+        if (tc < wc) {
+          wc = tc;
+          w = t;
+        }
+      }
+}
+
+__global__ void __launch_bounds__(THREADS) k_lr_spec(const FrameParams *fp, const uint8_t *cdef, const uint8_t *dbk,
+                                                    const uint8_t *src, Fit *fits) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Shared &sh = *reinterpret_cast<Shared *>(smem_raw);
+  const int gu = blockIdx.x;
+  int plane = 2;
+  while (plane > 0 && gu < fp->lr_unit_off[plane]) plane--;
+  const int u = gu - fp->lr_unit_off[plane];
+  Fit &F = fits[gu];
+  if (threadIdx.x == 0) {
+    unit_geom(fp, plane, u / fp->lr_unit_cols[plane], u % fp->lr_unit_cols[plane], &sh.geom);
+    sh.cn = F.n;
+  }
+  for (int i = threadIdx.x; i < F.n * 6; i += THREADS) sh.ctaps[i / 6][i % 6] = F.taps[i / 6][i % 6];
+  for (int i = threadIdx.x; i < F.n; i += THREADS) sh.csse[i] = F.sse[i];
+  __syncthreads();
+  const Geom g = sh.geom;
+  const int n0 = sh.cn;
+  int fitted[2][3], ref[2][3];
+  for (int pass = 0; pass < 2; pass++)
+    for (int j = 0; j < 3; j++) fitted[pass][j] = F.w[pass][j];
+  bool staged = false;
+  for (int q = 0; q < 3 && q <= u; q++) {
+    for (int pass = 0; pass < 2; pass++)
+      for (int j = 0; j < 3; j++) ref[pass][j] = q == 0 ? T(Wiener_Taps_Mid)[j] : fits[gu - q].w[pass][j];
+    spec_path(fp, plane, g, cdef, dbk, src, fitted, ref, sh, staged);
+  }
+  __syncthreads();
+  const int n1 = sh.cn;
+  for (int i = n0 * 6 + threadIdx.x; i < n1 * 6; i += THREADS) F.taps[i / 6][i % 6] = sh.ctaps[i / 6][i % 6];
+  for (int i = n0 + threadIdx.x; i < n1; i += THREADS) F.sse[i] = sh.csse[i];
+  if (threadIdx.x == 0) F.n = n1;
+}
+
 __global__ void __launch_bounds__(THREADS) k_lr_select(FrameParams *fp, const uint8_t *cdef, const uint8_t *dbk,
                                                       const uint8_t *src, const Fit *fits, LrUnit *units,
                                                       int lrTest, int *lrTypes) {
@@ -555,7 +664,13 @@ __global__ void __launch_bounds__(THREADS) k_lr_select(FrameParams *fp, const ui
   }
   int used = 0;
   for (int u = 0; u < nUnits; u++) {
-    const Fit &F = fits[off + u];
+    __syncthreads();  // every thread is done with the previous unit's copy
+    {  // the unit's first-pass results into shared memory (the rate scan reads them many times)
+      const int *fs = reinterpret_cast<const int *>(fits + off + u);
+      int *fd = reinterpret_cast<int *>(&sh.fit);
+      for (int k = threadIdx.x; k < (int)(sizeof(Fit) / 4); k += THREADS) fd[k] = fs[k];
+    }
+    const Fit &F = sh.fit;
     Geom g;
     if (threadIdx.x == 0) unit_geom(fp, plane, u / fp->lr_unit_cols[plane], u % fp->lr_unit_cols[plane], &sh.geom);
     __syncthreads();

@@ -431,6 +431,7 @@ extern "C" int mav1cu_session_create(int width, int height, int max_cdef_presets
   cudaFuncSetAttribute(ana::k_analyze_level, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ANA_SMEM(16));
   cudaFuncSetAttribute(lrs::k_lr_fit, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(lrs::Shared));
   cudaFuncSetAttribute(lrs::k_lr_select, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(lrs::Shared));
+  cudaFuncSetAttribute(lrs::k_lr_spec, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(lrs::Shared));
   *out = s;
   return MAV1CU_OK;
 }
@@ -787,6 +788,12 @@ extern "C" int mav1cu_lr_search(mav1cu_session *s, int lr_test) {
                                                                        U8(s, MAV1CU_BUF_DBK), U8(s, MAV1CU_BUF_SRC),
                                                                        s->lrfit);
   if (after_launch(s, "loop-restoration fit")) return s->err;
+  // the refinement's candidates under guessed references, for all units at
+  // once: the serial choice below finds most of its SSEs cached
+  lrs::k_lr_spec<<<n, lrs::THREADS, sizeof(lrs::Shared), s->stream>>>(DP(s), U8(s, MAV1CU_BUF_REC),
+                                                                        U8(s, MAV1CU_BUF_DBK), U8(s, MAV1CU_BUF_SRC),
+                                                                        s->lrfit);
+  if (after_launch(s, "loop-restoration speculative refinement")) return s->err;
   lrs::k_lr_select<<<3, lrs::THREADS, sizeof(lrs::Shared), s->stream>>>(
       (FrameParams *)s->buf[MAV1CU_BUF_PARAMS], U8(s, MAV1CU_BUF_REC), U8(s, MAV1CU_BUF_DBK), U8(s, MAV1CU_BUF_SRC),
       s->lrfit, (LrUnit *)s->buf[MAV1CU_BUF_LRUNITS], lr_test, s->lr_types);
@@ -1269,9 +1276,9 @@ extern "C" int mav1cu_stream_encode(mav1cu_stream *st, const mav1cu_frame_job *j
       return s->err;
     src = st->staging[ei][b];
   }
-  dim3 grid((s->g.stride[0] + 127) / 128, s->g.plane_h[0], 3);
-  drv::k_load_source<<<grid, 128, 0, s->stream>>>(src, U8(s, MAV1CU_BUF_SRC), c.width, c.height, s->g.sb_cols,
-                                                  s->g.sb_rows);
+  dim3 grid((s->g.stride[0] + 511) / 512, (s->g.plane_h[0] + drv::LS_ROWS - 1) / drv::LS_ROWS, 3);
+  drv::k_load_source<<<grid, dim3(32, drv::LS_ROWS), 0, s->stream>>>(src, U8(s, MAV1CU_BUF_SRC), c.width, c.height,
+                                                                    s->g.sb_cols, s->g.sb_rows);
   if (after_launch(s, "load source")) return s->err;
   if (b >= 0 && check_cuda(s, cudaEventRecord(st->load_done[ei][b], s->stream), "source upload")) return s->err;
   if (!job->is_key) {

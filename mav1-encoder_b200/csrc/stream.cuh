@@ -317,8 +317,6 @@ static void frame_params(const Norm &n, const mav1cu_frame_job &j, FrameParams *
   *presets = cdefOff ? 0 : (nPresets ? 1 << fp->cdef_bits : 0);
 }
 
-// Packed I420 -> padded planes with right / bottom edge replication
-// (load_source, encoder.c:297-310).
 // Stores frame parameters passed by value (the launch copies them).
 __global__ void k_store_params(FrameParams fp, FrameParams *dst) {
   const int *a = (const int *)&fp;
@@ -326,15 +324,36 @@ __global__ void k_store_params(FrameParams fp, FrameParams *dst) {
   for (int k = threadIdx.x; k < (int)(sizeof(FrameParams) / 4); k += blockDim.x) d[k] = a[k];
 }
 
-__global__ void k_load_source(const uint8_t *i420, uint8_t *dst, int w, int h, int sbCols, int sbRows) {
+// load_source (encoder.c:297-310): the I420 picture into the padded planar
+// layout, the right and bottom edges replicated up to the superblock-aligned
+// size. A thread writes 16 consecutive samples of a row as one 16-byte store
+// (padded rows are multiples of 32 samples, plane offsets multiples of 1024)
+// and reads them as one 16-byte load where the source run is aligned and
+// inside the row, byte by byte with the edge clamp otherwise. CTAs of 32 x 8
+// threads cover 512 samples of 8 rows; blockIdx.z is the plane.
+constexpr int LS_ROWS = 8;
+__global__ void __launch_bounds__(256) k_load_source(const uint8_t *i420, uint8_t *dst, int w, int h, int sbCols,
+                                                     int sbRows) {
   int p = blockIdx.z;
   int pw = p ? (w + 1) >> 1 : w, ph = p ? (h + 1) >> 1 : h;
   int aw = p ? sbCols * 32 : sbCols * 64, ah = p ? sbRows * 32 : sbRows * 64;
-  int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+  int x = (blockIdx.x * 32 + threadIdx.x) * 16, y = blockIdx.y * LS_ROWS + threadIdx.y;
   if (x >= aw || y >= ah) return;
   size_t planeOff = p == 0 ? 0 : (size_t)w * h + (size_t)(p - 1) * ((w + 1) >> 1) * ((h + 1) >> 1);
   size_t dstOff = p == 0 ? 0 : (size_t)sbCols * 64 * sbRows * 64 + (size_t)(p - 1) * sbCols * 32 * sbRows * 32;
-  dst[dstOff + (size_t)y * aw + x] = i420[planeOff + (size_t)imin(y, ph - 1) * pw + imin(x, pw - 1)];
+  const uint8_t *row = i420 + planeOff + (size_t)imin(y, ph - 1) * pw;
+  uint4 v;
+  if (x + 16 <= pw && (((uintptr_t)(row + x)) & 15) == 0) {
+    v = *(const uint4 *)(row + x);
+  } else {
+    uint8_t b[16];
+#pragma unroll
+    for (int k = 0; k < 16; k++) b[k] = row[imin(x + k, pw - 1)];
+    v = make_uint4(b[0] | b[1] << 8 | b[2] << 16 | (unsigned)b[3] << 24, b[4] | b[5] << 8 | b[6] << 16 | (unsigned)b[7] << 24,
+                   b[8] | b[9] << 8 | b[10] << 16 | (unsigned)b[11] << 24,
+                   b[12] | b[13] << 8 | b[14] << 16 | (unsigned)b[15] << 24);
+  }
+  *(uint4 *)(dst + dstOff + (size_t)y * aw + x) = v;
 }
 
 }  // namespace drv
