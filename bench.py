@@ -46,6 +46,12 @@ import numpy as np
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "mav1-encoder_b200"))
+# Every encoder runs several CUDA streams (two frame engines, their transfer,
+# upload and status streams); with the default 8 hardware work queues they
+# alias and serialise. Read when the CUDA context is created, so set here,
+# before anything touches the device (measured: the 16-stream batch 766 ->
+# 786 fps, the clip through the API 970 -> 980 fps).
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
 
 import synthetic  # noqa: E402
 
