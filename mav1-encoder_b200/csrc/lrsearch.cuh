@@ -73,25 +73,36 @@ HD int unit_col_of(const FrameParams *fp, int plane, int c) {
   return imin(fp->lr_unit_cols[plane] - 1, ((c * MI_SIZE) >> (plane > 0)) / fp->lr_unit_size[plane]);
 }
 
+// First r in [0, n) with of(r) >= v, or n: unit_row_of / unit_col_of are
+// non-decreasing in r (a clamped quotient of a growing numerator).
+template <typename F>
+__device__ __forceinline__ int first_at_least(int n, int v, F of) {
+  int lo = 0, hi = n;
+  while (lo < hi) {
+    int mid = (lo + hi) >> 1;
+    if (of(mid) >= v) hi = mid;
+    else lo = mid + 1;
+  }
+  return lo;
+}
+
+// The 4x4 rows and columns whose unit is (ur, uc): the contiguous run of r
+// with unit_row_of(r) == ur (and the same for columns), found by binary
+// search since the maps are non-decreasing; an empty run leaves
+// r0 = rows4, r1 = 0 (c0 = cols4, c1 = 0).
 __device__ void unit_geom(const FrameParams *fp, int plane, int ur, int uc, Geom *g) {
   int rows4 = (fp->frame_h + 3) >> 2, cols4 = (fp->frame_w + 3) >> 2;
   g->plane = plane;
   g->ur = ur;
   g->uc = uc;
-  g->r0 = rows4;
-  g->r1 = 0;
-  g->c0 = cols4;
-  g->c1 = 0;
-  for (int r = 0; r < rows4; r++)
-    if (unit_row_of(fp, plane, r) == ur) {
-      g->r0 = imin(g->r0, r);
-      g->r1 = r + 1;
-    }
-  for (int c = 0; c < cols4; c++)
-    if (unit_col_of(fp, plane, c) == uc) {
-      g->c0 = imin(g->c0, c);
-      g->c1 = c + 1;
-    }
+  auto rowOf = [&](int r) { return unit_row_of(fp, plane, r); };
+  auto colOf = [&](int c) { return unit_col_of(fp, plane, c); };
+  int r0 = first_at_least(rows4, ur, rowOf), r1 = first_at_least(rows4, ur + 1, rowOf);
+  int c0 = first_at_least(cols4, uc, colOf), c1 = first_at_least(cols4, uc + 1, colOf);
+  g->r0 = r0 < r1 ? r0 : rows4;
+  g->r1 = r0 < r1 ? r1 : 0;
+  g->c0 = c0 < c1 ? c0 : cols4;
+  g->c1 = c0 < c1 ? c1 : 0;
 }
 
 // A unit's samples staged in shared memory: the CDEF output, the deblocked
