@@ -12,7 +12,9 @@
 // rows on packed bytes with __vsadu4; interior candidates read unaligned
 // words through funnel shifts), and the warp reduces the 64-bit key
 // (cost << 32 | index) with shuffles, which yields exactly the serial first
-// minimum. Sub-pel candidates x 4x4 units are spread over the lanes and
+// minimum. The 64x64 level has few nodes: a CTA per node, its four warps
+// taking candidates in turn and each warp's lanes splitting a candidate's
+// byte pairs. Sub-pel candidates x 4x4 units are spread over the lanes and
 // summed in shared memory. Quarter-pel planes (16 per reference, EIGHTTAP,
 // the T_ME_HPEL mode) are built once per reference picture by their own
 // kernel, one thread per sample.
@@ -247,6 +249,55 @@ __device__ int full_cost(const Frame &f, const Node &m, int dy, int dx) {
   return full_sad(f, m, dy, dx, rs) + fp->ac_q[0] * bits / 64;
 }
 
+// The same cost with the warp's 32 lanes splitting one candidate's byte pairs
+// (the 64x64 level: few nodes, so each CTA's four warps take candidates in
+// turn instead of one thread a candidate). Every lane returns the total. The
+// sums are the ones full_sad / dec_sad form, in another order: unsigned
+// integer addition, so the cost is the same.
+// Not inlined, with its arguments by value: the kernel's other levels keep
+// their registers (inlined, the kernel spills at its 96-register bound).
+__device__ __noinline__ int warp_full_cost(const FrameParams *fp, const uint8_t *fsrc, const uint8_t *fref,
+                                           const uint8_t *dsrc, const uint8_t *dref, int x, int y, int w, int step,
+                                           int dy, int dx, int lane) {
+  int bits = 2 + 2 * floor_log2(iabs(dy) * 8 + 1) + 2 * floor_log2(iabs(dx) * 8 + 1);
+  unsigned sad = 0;
+  int scale;
+  if ((fp->turbo & T_ME_DEC) && step >= ME_COARSE_STEP) {
+    // dec_sad: n x n pairs of the decimated planes, lanes along rows
+    int W = dec_w(fp), H = dec_h(fp), lg = floor_log2(w >> 2), n = 1 << lg;
+    int x0 = x >> 2, y0 = y >> 2, oy = dy >> 2, ox = dx >> 2;
+    for (int p = lane; p < n * n; p += 32) {
+      int i = p >> lg, j = p & (n - 1);
+      int sy = imin(y0 + i, H - 1), ry = clip3(0, H - 1, y0 + i + oy);
+      sad = __sad((int)dsrc[sy * W + imin(x0 + j, W - 1)], (int)dref[ry * W + clip3(0, W - 1, x0 + j + ox)], sad);
+    }
+    scale = 16;
+  } else {
+    // full_sad: rows 0, rs, 2 rs, ... of w / 4 words, lanes along rows
+    int rs = (fp->turbo & T_ME_RSUB) && step == 1 ? 2 : 1;
+    int stride = fp->stride[0], W = fp->frame_w, Hh = fp->frame_h;
+    const uint8_t *src = fsrc + fp->offset[0], *ref = fref + fp->offset[0];
+    int lgw = floor_log2(w >> 2), nw = (w / rs) << lgw;
+    if (x + dx >= 0 && x + dx + w <= W && y + dy >= 0 && y + dy + w <= Hh) {
+      for (int q = lane; q < nw; q += 32) {
+        int i = (q >> lgw) * rs, j = q & ((1 << lgw) - 1);
+        uint32_t s = __ldg((const uint32_t *)(src + (y + i) * stride + x) + j);
+        sad = __vsadu4(s, load_u32_unaligned(ref + (y + i + dy) * stride + x + dx + 4 * j)) + sad;
+      }
+    } else {
+      for (int q = lane; q < nw; q += 32) {
+        int i = (q >> lgw) * rs, j = q & ((1 << lgw) - 1);
+        const uint8_t *s = src + (y + i) * stride + x + 4 * j;
+        const uint8_t *r = ref + clip3(0, Hh - 1, y + i + dy) * stride;
+        for (int b = 0; b < 4; b++) sad = __sad((int)s[b], (int)r[clip3(0, W - 1, x + 4 * j + b + dx)], sad);
+      }
+    }
+    scale = rs;
+  }
+  for (int off = 16; off > 0; off >>= 1) sad += __shfl_xor_sync(0xffffffffu, sad, off);
+  return (int)sad * scale + fp->ac_q[0] * bits / 64;
+}
+
 // SATD of 4x4 unit u of the node against the quarter-pel plane prediction at
 // (mvr, mvc) (even, 1/8 units) (k_me.h:317-340).
 __device__ int unit_satd_hp(const Frame &f, const Node &m, int mvr, int mvc, int u) {
@@ -385,11 +436,22 @@ __global__ void __launch_bounds__(128, MAV1CU_ME_MIN_CTAS) k_me_level(Frame f0, 
       WORK(dec ? W_ME_DSAD : W_ME_SAD, (long long)m.count * (dec ? (m.w >> 2) * (m.w >> 2) : (m.w / rs) * m.w));
     }
     unsigned long long best = ~0ull;
-    for (int k = grp.rank; k < m.count; k += grp.size) {
-      int dy, dx;
-      candidate(m, k, &dy, &dx);
-      unsigned long long key = ((unsigned long long)(unsigned)full_cost(f, m, dy, dx) << 32) | (unsigned)k;
-      best = key < best ? key : best;
+    if (whole_cta) {
+      // a warp per candidate, every lane holding the warp's running minimum
+      for (int k = warp; k < m.count; k += 4) {
+        int dy, dx;
+        candidate(m, k, &dy, &dx);
+        int cost = warp_full_cost(fp, f.src, f.ref, f.dsrc, f.dref, m.x, m.y, m.w, m.step, dy, dx, lane);
+        unsigned long long key = ((unsigned long long)(unsigned)cost << 32) | (unsigned)k;
+        best = key < best ? key : best;
+      }
+    } else {
+      for (int k = grp.rank; k < m.count; k += grp.size) {
+        int dy, dx;
+        candidate(m, k, &dy, &dx);
+        unsigned long long key = ((unsigned long long)(unsigned)full_cost(f, m, dy, dx) << 32) | (unsigned)k;
+        best = key < best ? key : best;
+      }
     }
     best = group_min(best, grp);
     if (whole_cta) {
