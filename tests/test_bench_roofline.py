@@ -1,7 +1,10 @@
 """The bench's roofline arithmetic on CPU: the dominant kernel's bytes over
 its stage time against the HBM peak, and the counted integer operations of
 every stage (units x operations per unit) over the stage time against the
-measured integer peak. Synthetic timings and counts; no GPU."""
+measured integer peak. Synthetic timings and counts; no GPU. Also the
+bench's clock record (median and maximum SM clock, throttle reasons seen
+active) from fake nvidia-smi samples, and the split of the benchmark clip's
+coding plan into closed GOPs that the bench codes concurrently."""
 import os
 import sys
 
@@ -49,3 +52,29 @@ def test_hbm_roofline_of_the_key_frame_recon():
     assert r["ms_per_launch"] == 8.0 and r["int_ops"]["stages"]
     assert bench.roofline(None, peaks) is None
     assert bench.roofline(TIMES, {}, None)["peak_source"] == "fallback"
+
+
+def test_clock_summary_reads_median_max_and_active_reasons():
+    c = bench.Clocks(0)
+    c.samples = [["1965", "1965", "700.1", "Not Active", "Not Active", "Not Active", "Not Active"],
+                 ["1900", "1965", "990.0", "Not Active", "Not Active", "Not Active", "Active"],
+                 ["1950", "1965", "980.5", "Not Active", "Not Active", "Not Active", "Not Active"],
+                 ["[N/A]", "1965", "1.0", "", "", "", ""]]
+    s = c.summary()
+    assert s == {"sm_mhz": 1950.0, "sm_max_mhz": 1965.0, "reasons": ["sw_power_cap"], "samples": 3}
+    c.samples = [["1965", "1965", "900", "Active", "Not Active", "Active", "Not Active"]]
+    assert c.summary()["reasons"] == ["hw_slowdown", "sw_thermal_slowdown"]
+    assert bench.Clocks(0).summary() == {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+
+
+def test_benchmark_clip_splits_into_two_closed_gops():
+    import mav1cu
+    cfg = mav1cu.cli_config(bench.SPEC.width, bench.SPEC.height, **bench.FLAGS)
+    jobs = mav1cu.plan(cfg, bench.SPEC.frames)
+    gops = bench.split_gops(jobs)
+    assert len(gops) == 2
+    for g in gops:
+        assert g[0]["is_key"] and not any(j["is_key"] for j in g[1:])
+    shown = sorted(int(j["disp"]) for g in gops for j in g)
+    assert shown == sorted(set(shown)) and shown[0] == 0 and shown[-1] == bench.SPEC.frames - 1
+    assert {int(j["disp"]) for j in gops[1]} == set(range(60, 120))
