@@ -149,3 +149,17 @@ def test_forward_matrices_identical_from_concurrent_threads():
     for t in th:
         t.join()
     assert all(np.array_equal(m, want) for ms in out for m in ms)
+
+
+def test_api_ivf_container_equals_the_reference_cli_container():
+    """mav1api.ivf_bytes (the container the bench and the API tests hash)
+    equals the oracle's, which the oracle tests pin to the reference CLI's
+    own output file byte for byte."""
+    import mav1api
+    rng = np.random.default_rng(9)
+    packets = [rng.integers(0, 256, int(n), dtype=np.uint8).tobytes() for n in rng.integers(1, 5000, 17)]
+    for (w, h) in ((1920, 1080), (203, 131), (64, 48)):
+        a = mav1api.ivf_bytes(packets, w, h)
+        assert a == oracle.ivf_bytes(packets, w, h)
+        assert a[:4] == b"DKIF" and int.from_bytes(a[24:28], "little") == len(packets)
+    assert mav1api.ivf_bytes([], 64, 48) == oracle.ivf_bytes([], 64, 48)
